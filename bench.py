@@ -1,0 +1,415 @@
+"""Benchmark: the horizon march of the site-scale workload on B200.
+
+One step = the production horizon march (both DEM passes, primary 4096x4096
+at 5 m + regional 2000x2000 at 240 m, 200 km range) over one 128x128 tile with
+1440 azimuths = 23,592,960 rays.  Tiles rotate every step (row-major tiles of
+the primary DEM, rank r of N taking tiles r, r+N, ...: weak scaling, no data
+collective).  Inputs are seeded synthetic DEMs (fBm + craters) with the
+configuration's shapes; the per-step working set (segments 67 MB + DEM and
+pyramids 106 MB + output 94 MB) exceeds the 126 MB L2.
+
+value:  rays/s over all ranks with segments already resident in HBM (device
+        march + transpose, CUDA events on the launch stream, max over ranks).
+e2e:    rays/s through the drop-in CudaSession.subpatch_hierarchical_all_passes
+        call with pinned host buffers (segments H2D + slopes D2H every step).
+cpu_baseline: the oracle's C restatement of the march (all host threads) on a
+        bounded random sample of rays of the same tiles (rank 0, N=1 only).
+
+--impl reference: the reference algorithm's CPU restatement (oracle port; the
+reference has no CPU horizon path of its own) on the host cores, same metric.
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "horizon rays/s & lightmap px·steps/s, 1 B200: batched vs plain, adjoint/fwd"
+TILE = 128
+AZIMUTHS = 1440
+RAYS_PER_TILE = TILE * TILE * AZIMUTHS
+RANGE_M = 200_000.0
+OBSERVER_M = 0.0
+# Algorithmic FP32 flops (FMA = 2) per unit of the march, counted from the
+# reference source (cuda_backend.py:672-867): per ray step (two quartics,
+# planar distance, chord cubic, footprint, level choice, two tangents and
+# their reciprocals), per node visit (slab exit, fallback, near distance,
+# four-cell local-z bound, step) and per level-0 sample (bilinear, local-z
+# slope, tangent norm and the adaptive step rule).
+FLOPS_PER_STEP = 67
+FLOPS_PER_VISIT = 31
+FLOPS_PER_SAMPLE = 35
+# Bytes a node visit gathers (4 float32 cells) and a level-0 sample adds.
+BYTES_PER_VISIT = 16
+BYTES_PER_SAMPLE = 16
+
+
+def log(*args):
+    print(*args, file=sys.stderr, flush=True)
+
+
+def dist_env():
+    rank = int(os.environ.get("RANK", "0"))
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return rank, world, local
+
+
+def workload_config():
+    return {
+        "workload": "site-scale horizon march: 128x128 tile x 1440 az, 2 DEM passes",
+        "primary_dem": "4096x4096 f32 @ 5 m, fBm sigma 150 m H 0.8 + 600 craters <= 8 km",
+        "regional_dem": "2000x2000 f32 @ 240 m, fBm sigma 1.2 km + 2 km tilt",
+        "range_km": RANGE_M / 1000.0,
+        "azimuths": AZIMUTHS,
+        "rays_per_step": RAYS_PER_TILE,
+        "l2": "inputs larger than L2 (67 MB segments + 106 MB DEMs/pyramids + 94 MB "
+              "output per step), tile changes every step",
+    }
+
+
+def tile_schedule(rank, world, count):
+    tiles_per_side = 4096 // TILE
+    # Start in the DEM interior so every step is a full tile with long rays.
+    order = [(ty, tx) for ty in range(4, tiles_per_side - 4) for tx in range(4, tiles_per_side - 4)]
+    rng = np.random.default_rng(1234)
+    rng.shuffle(order)
+    picked = [order[(rank + k * world) % len(order)] for k in range(count)]
+    return [(ty * TILE, tx * TILE) for ty, tx in picked]
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle samples during the timed region."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.device_index = device_index
+        self.proc = None
+        self.lines: list[str] = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.device_index}", f"--query-gpu={self.QUERY}",
+                 "--format=csv,noheader,nounits", "-lms", "200"],
+                stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.thread.join(timeout=2)
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                mx = float(parts[2])
+            except ValueError:
+                continue
+            for name, flag in zip(names, parts[5:9]):
+                if flag.lower().startswith("active"):
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def build_dems():
+    from lunarscout_b200.synthetic import regional_dem, site_dem
+
+    started = time.perf_counter()
+    primary = site_dem()
+    regional = regional_dem()
+    log(f"[bench] synthetic DEMs in {time.perf_counter() - started:.1f}s")
+    return primary, regional
+
+
+def cpu_sample_rate(primary, regional, tiles, seconds_target=12.0, threads=None):
+    """Oracle march throughput (rays/s) on a bounded random ray sample."""
+    import oracle
+    from oracle import segments as oseg
+    from lunarscout_b200.contract import PyramidArrays, map_parameters, projection_parameters
+
+    pyramids = []
+    for dem in (primary, regional):
+        mips, levels = oracle.build_pyramid(dem.elevation_m)
+        pyramids.append(PyramidArrays(dem.elevation_m, mips, levels, map_parameters(dem),
+                                      projection_parameters(dem)))
+    threads = threads or oracle.default_threads()
+    tile_row, tile_column = tiles[0]
+    segments = oseg.build_segments([primary, regional], tile_column=tile_column,
+                                   tile_row=tile_row, tile_width=TILE, azimuth_count=AZIMUTHS,
+                                   maximum_distance_m=RANGE_M, observer_elevation_m=OBSERVER_M,
+                                   threads=threads)
+    rng = np.random.default_rng(7)
+    count = 256
+    elapsed = 0.0
+    rays = 0
+    while elapsed < seconds_target:
+        pixels = rng.integers(0, TILE * TILE, size=count).astype(np.int32)
+        azimuths = rng.integers(0, AZIMUTHS, size=count).astype(np.int32)
+        started = time.perf_counter()
+        oracle.march_all_passes(segments, pyramids, tile_column=tile_column, tile_row=tile_row,
+                                observer_elevation_m=OBSERVER_M, pixels=pixels,
+                                azimuths=azimuths, threads=threads)
+        took = time.perf_counter() - started
+        elapsed += took
+        rays += count
+        if took < 1.0:
+            count *= 4
+    return rays / elapsed, threads, rays, elapsed
+
+
+def run_reference(args):
+    rank, world, _ = dist_env()
+    if rank != 0:
+        return
+    primary, regional = build_dems()
+    tiles = tile_schedule(0, 1, 1)
+    per_step = []
+    rates = []
+    for step in range(args.warmup + args.steps):
+        rate, threads, rays, elapsed = cpu_sample_rate(primary, regional, tiles,
+                                                       seconds_target=args.reference_seconds)
+        if step >= args.warmup:
+            rates.append(rate)
+            per_step.append(elapsed)
+    value = statistics.median(rates)
+    line = {
+        "impl": "reference",
+        "metric": METRIC, "value": value, "unit": "rays/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": 1000.0 * RAYS_PER_TILE / value,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic",
+        "config": workload_config(),
+        "cpu_baseline": {"value": value, "unit": "rays/s", "cores": threads, "kind": "port",
+                         "sample": f"random rays of a site-scale tile, both DEM passes, "
+                                   f"~{args.reference_seconds:.0f} s of CPU work per step"},
+        "e2e": {"value": value, "unit": "rays/s", "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args):
+    import torch
+    import torch.distributed as dist
+
+    rank, world, local = dist_env()
+    torch.cuda.set_device(local)
+    if world > 1:
+        from datetime import timedelta
+
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300),
+                                device_id=torch.device("cuda", local))
+    from lunarscout_b200.cuda_backend import CudaSession
+    from lunarscout_b200._native import pinned_empty
+
+    primary, regional = build_dems()
+    session = CudaSession(local)
+    stream = torch.cuda.current_stream()
+    session.set_stream(stream.cuda_stream)
+    dems = [session.upload_dem_grid(primary), session.upload_dem_grid(regional)]
+    centers = (TILE // 8 + 2) ** 2
+    total_steps = args.warmup + args.steps
+    tiles = tile_schedule(rank, world, total_steps)
+    segment_shape = (AZIMUTHS, centers, 2, 18)
+    segments = []
+    started = time.perf_counter()
+    for tile_row, tile_column in tiles:
+        buffer = torch.empty(segment_shape, dtype=torch.float32, device="cuda")
+        session.generate_segments_device(dems, buffer.data_ptr(), tile_column=tile_column,
+                                         tile_row=tile_row, azimuth_count=AZIMUTHS,
+                                         maximum_distance_m=RANGE_M,
+                                         observer_elevation_m=OBSERVER_M)
+        segments.append(buffer)
+    torch.cuda.synchronize()
+    segment_seconds = (time.perf_counter() - started) / total_steps
+    output = torch.empty((TILE * TILE, AZIMUTHS), dtype=torch.float32, device="cuda")
+
+    def step(k, pass_seconds=None):
+        tile_row, tile_column = tiles[k]
+        session.march_all_passes_device(segments[k].data_ptr(), AZIMUTHS, centers, dems,
+                                        tile_column=tile_column, tile_row=tile_row,
+                                        observer_elevation_m=OBSERVER_M,
+                                        device_out=output.data_ptr(), pass_seconds=pass_seconds)
+
+    # Algorithmic work of the timed tiles: one counted (diagnostic) launch each.
+    session.set_counting(True)
+    visits = samples = ray_steps = 0
+    for k in range(args.warmup, total_steps):
+        step(k)
+        torch.cuda.synchronize()
+        v, s, n = session.last_counters()
+        visits, samples, ray_steps = visits + v, samples + s, ray_steps + n
+    session.set_counting(False)
+
+    for k in range(args.warmup):
+        step(k)
+    torch.cuda.synchronize()
+
+    sampler = ClockSampler(local)
+    if world > 1:
+        dist.barrier()
+    torch.cuda.synchronize()
+    sampler.start()
+    time.sleep(0.3)
+    start_event = torch.cuda.Event(enable_timing=True)
+    end_event = torch.cuda.Event(enable_timing=True)
+    pass_times = []
+    start_event.record(stream)
+    for k in range(args.warmup, total_steps):
+        seconds = np.zeros(2, dtype=np.float64)
+        step(k, seconds)
+        pass_times.append(seconds)
+    end_event.record(stream)
+    torch.cuda.synchronize()
+    clocks = sampler.stop()
+    elapsed = start_event.elapsed_time(end_event) / 1000.0
+    if world > 1:
+        t = torch.tensor([elapsed], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        elapsed = float(t.item())
+        dist.barrier()
+    rays = world * args.steps * RAYS_PER_TILE
+    value = rays / elapsed
+
+    # End to end through the drop-in session call with pinned host buffers.
+    e2e_value = None
+    h2d = int(np.prod(segment_shape)) * 4
+    d2h = TILE * TILE * AZIMUTHS * 4
+    from lunarscout_b200.contract import PyramidArrays
+
+    class _Pyr:  # the session's resident-pyramid cache keys on identity
+        pass
+
+    e2e_session = CudaSession(local)
+    host_pyramids = []
+    for dem in (primary, regional):
+        p = e2e_session.build_max_pyramid(dem)
+        host_pyramids.append(p)
+    host_segments = [pinned_empty(segment_shape, np.float32) for _ in range(2)]
+    for i in range(2):
+        host_segments[i][...] = segments[args.warmup + i].cpu().numpy()
+    e2e_session.subpatch_hierarchical_all_passes(host_segments[0], host_pyramids,
+                                                 tile_column=tiles[args.warmup][1],
+                                                 tile_row=tiles[args.warmup][0],
+                                                 tile_width=TILE, tile_height=TILE,
+                                                 subpatch_size=8)
+    e2e_steps = max(2, min(args.steps, 6))
+    if world > 1:
+        dist.barrier()
+    started = time.perf_counter()
+    for k in range(e2e_steps):
+        index = args.warmup + (k % 2)
+        e2e_session.subpatch_hierarchical_all_passes(
+            host_segments[k % 2], host_pyramids, tile_column=tiles[index][1],
+            tile_row=tiles[index][0], tile_width=TILE, tile_height=TILE, subpatch_size=8)
+    e2e_elapsed = time.perf_counter() - started
+    if world > 1:
+        t = torch.tensor([e2e_elapsed], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_elapsed = float(t.item())
+    e2e_value = world * e2e_steps * RAYS_PER_TILE / e2e_elapsed
+    e2e_session.close()
+
+    fp32_peak = session.fp32_probe()
+    pass_times = np.array(pass_times)
+    march_seconds = float(pass_times.sum()) / (2 * args.steps)  # per launch
+    flops = (FLOPS_PER_STEP * ray_steps + FLOPS_PER_VISIT * visits
+             + FLOPS_PER_SAMPLE * samples) / (2 * args.steps)
+    achieved = flops / march_seconds / 1e12
+    gathered = (BYTES_PER_VISIT * visits + BYTES_PER_SAMPLE * samples) / (2 * args.steps)
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.skip_cpu:
+        rate, threads, rays_cpu, secs = cpu_sample_rate(primary, regional, tiles[args.warmup:],
+                                                        seconds_target=args.cpu_seconds)
+        cpu = {"value": rate, "unit": "rays/s", "cores": threads, "kind": "port",
+               "sample": f"{rays_cpu} random rays of the first timed tile, both DEM passes "
+                         f"({secs:.1f} s)"}
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "rays/s", "n_gpus": world,
+            "steps": args.steps, "warmup": args.warmup,
+            "ms_per_step": 1000.0 * elapsed / args.steps,
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "dtype": "f32", "data": "synthetic",
+            "config": workload_config(),
+            "roofline": {
+                "bound": "fp32", "kernel": "march_pass_kernel",
+                "achieved": achieved, "peak": fp32_peak, "unit": "TFLOP/s",
+                "frac": achieved / fp32_peak,
+                "peak_source": "FP32 FMA probe measured in this run (no FP32 entry in "
+                               "MEASURED_PEAKS.json)",
+                "traffic": None,
+                "algorithmic_flops_per_launch": flops,
+                "gathered_bytes_per_launch": gathered,
+                "launch_ms": march_seconds * 1000.0,
+                "node_visits_per_ray": visits / (args.steps * RAYS_PER_TILE),
+            },
+            "cpu_baseline": cpu,
+            "e2e": {"value": e2e_value, "unit": "rays/s", "h2d_bytes_per_step": h2d,
+                    "d2h_bytes_per_step": d2h},
+            "gpu_launches": 3 * args.steps,
+            "clocks": clocks,
+            "segment_generation_ms_per_tile": segment_seconds * 1000.0,
+        }
+        print(json.dumps(line), flush=True)
+    session.close()
+    if world > 1:
+        dist.destroy_process_group()
+
+
+def main():
+    parser = argparse.ArgumentParser()
+    parser.add_argument("--gpus", type=int, default=1)
+    parser.add_argument("--steps", type=int, default=10)
+    parser.add_argument("--warmup", type=int, default=3)
+    parser.add_argument("--impl", choices=("ours", "reference"), default="ours")
+    parser.add_argument("--cpu-seconds", type=float, default=12.0)
+    parser.add_argument("--reference-seconds", type=float, default=8.0)
+    parser.add_argument("--skip-cpu", action="store_true")
+    args = parser.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()

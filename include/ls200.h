@@ -1,0 +1,144 @@
+/*
+ * ls200 — C ABI of the B200-native lunarscout horizon-and-lighting hot path.
+ *
+ * Every entry point returns an ls200_status; on failure a message is kept per
+ * calling thread (ls200_last_error).  No C++ exception crosses this boundary.
+ * Host pointers are plain C arrays in the reference's layouts; "_device"
+ * entry points take device pointers and a cudaStream_t passed as void*.
+ * Calls on one context are serialised by the context's own lock, so a
+ * context may be shared between threads; the GIL is released by ctypes.
+ *
+ * Each entry point names the reference interface it replaces
+ * (paths within Costigan/lunarscout).
+ */
+#ifndef LS200_H
+#define LS200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+    LS200_OK = 0,
+    LS200_ERR_INVALID = 1,     /* input contract violated (Python: ValueError) */
+    LS200_ERR_CUDA = 2,        /* CUDA runtime failure during execution */
+    LS200_ERR_UNAVAILABLE = 3, /* no usable sm_100 device (CudaBackendError) */
+    LS200_ERR_TIMEOUT = 4,     /* a bounded device wait gave up */
+} ls200_status;
+
+typedef struct ls200_context ls200_context;
+typedef struct ls200_dem ls200_dem;
+
+/* Message of the last failed call made by this thread ("" if none). */
+const char *ls200_last_error(void);
+/* Library/ABI version, e.g. 1. */
+int ls200_abi_version(void);
+
+/* ---- context: src/lunarscout/_numba_horizon/cuda_backend.py:1157-1196
+ *      (CudaSession.__init__, .info) ---- */
+ls200_status ls200_context_create(int device_id, ls200_context **out);
+ls200_status ls200_context_destroy(ls200_context *ctx);
+ls200_status ls200_device_info(ls200_context *ctx, char *name, int name_capacity,
+                               int *major, int *minor, int *sm_count);
+/* Use `stream` (a cudaStream_t) for all later work of this context; NULL
+ * restores the context's own stream. */
+ls200_status ls200_set_stream(ls200_context *ctx, void *stream);
+ls200_status ls200_synchronize(ls200_context *ctx);
+
+/* ---- max pyramid: src/lunarscout/_numba_horizon/pyramid.py:19-31
+ *      (_level_layout) and cuda_backend.py:1260-1281 (build_max_pyramid) ---- */
+/* Writes up to `capacity` rows of (level, offset, width, height); returns the
+ * level count through *level_count and the mip element count. */
+ls200_status ls200_pyramid_layout(int width, int height, int32_t *levels, int capacity,
+                                  int *level_count, int64_t *mip_count);
+/* host level0 [height, width] -> host mips [mip_count] */
+ls200_status ls200_build_max_pyramid(ls200_context *ctx, const float *level0, int width,
+                                     int height, float *mips);
+
+/* ---- device-resident DEM (pyramid + georeference):
+ *      cuda_backend.py:1231-1258 (_prepare_production_pyramids) ---- */
+/* Uploads level0 and, if `mips` is NULL, builds the pyramid on the device.
+ * geo_transform: GDAL order (6 f64).  projection: radius, lat0, lon0, scale,
+ * false_easting, false_northing (6 f64).  map_parameters: the reference's 11
+ * float32 map parameters (pyramid.py:84-95). */
+ls200_status ls200_dem_create(ls200_context *ctx, const float *level0, int width, int height,
+                              const float *mips, const double *geo_transform,
+                              const double *projection, const float *map_parameters,
+                              ls200_dem **out);
+ls200_status ls200_dem_destroy(ls200_dem *dem);
+/* Copies the device mips back (e.g. to write a .pyr.bin cache). */
+ls200_status ls200_dem_download_mips(ls200_dem *dem, float *mips, int64_t capacity);
+
+/* ---- ray segments: src/lunarscout/_numba_horizon/geometry.py:575-673
+ *      (build_subpatch_segments_numba) and geometry_numba.py:142-364 ---- */
+/* Fills segments [azimuth_count, (tile_width/subpatch+2)^2, dem_count, 18]. */
+ls200_status ls200_segments(ls200_context *ctx, ls200_dem *const *dems, int dem_count,
+                            int tile_column, int tile_row, int tile_width, int azimuth_count,
+                            double maximum_distance_m, double observer_elevation_m,
+                            int subpatch_size, float *segments);
+ls200_status ls200_segments_device(ls200_context *ctx, ls200_dem *const *dems, int dem_count,
+                                   int tile_column, int tile_row, int tile_width,
+                                   int azimuth_count, double maximum_distance_m,
+                                   double observer_elevation_m, int subpatch_size,
+                                   float *device_segments);
+
+/* ---- horizon march: cuda_backend.py:1390-1443 (subpatch_hierarchical_pass)
+ *      and :1445-1552 (subpatch_hierarchical_all_passes) ---- */
+/* One pass; slopes [tile_width*tile_height, azimuth_count] pixel-major are the
+ * carried input (NULL = all -inf) and the output. */
+ls200_status ls200_march_pass(ls200_context *ctx, const float *segments, int azimuth_count,
+                              int center_count, int dem_count, const ls200_dem *primary,
+                              const ls200_dem *active, int tile_column, int tile_row,
+                              int tile_width, int tile_height, int subpatch_size,
+                              int pass_index, float observer_elevation_m,
+                              const float *slopes_in, float *slopes_out);
+/* Every pass on one resident slope buffer; pass_seconds[dem_count] receives
+ * CUDA-event kernel times (may be NULL). */
+ls200_status ls200_march_all_passes(ls200_context *ctx, const float *segments,
+                                    int azimuth_count, int center_count, int dem_count,
+                                    ls200_dem *const *dems, int tile_column, int tile_row,
+                                    int tile_width, int tile_height, int subpatch_size,
+                                    float observer_elevation_m, float *slopes,
+                                    double *pass_seconds);
+/* Device-resident variant: device_segments in, device_slopes out
+ * ([P, A] pixel-major slopes, or degrees when `degrees` is non-zero);
+ * pass_seconds as above (NULL skips the per-pass events and the wait). */
+ls200_status ls200_march_all_passes_device(ls200_context *ctx, const float *device_segments,
+                                           int azimuth_count, int center_count,
+                                           int dem_count, ls200_dem *const *dems,
+                                           int tile_column, int tile_row, int tile_width,
+                                           int tile_height, int subpatch_size,
+                                           float observer_elevation_m, float *device_out,
+                                           int degrees, double *pass_seconds);
+/* Node visits (inner hierarchy iterations), level-0 samples and ray steps
+ * (outer iterations) counted by the last march call of this context, when
+ * counting was enabled with ls200_set_counting (a slower diagnostic build of
+ * the kernel runs meanwhile). */
+ls200_status ls200_set_counting(ls200_context *ctx, int enabled);
+ls200_status ls200_last_counters(ls200_context *ctx, int64_t *visits, int64_t *samples,
+                                 int64_t *steps);
+
+/* slope -> degrees, float32(atan(s) * float32(180/pi)), -inf preserved:
+ * src/lunarscout/_numba_horizon/contract.py:362-371 (HorizonBuffers.degrees) */
+ls200_status ls200_slopes_to_degrees(ls200_context *ctx, const float *slopes, int64_t count,
+                                     float *degrees);
+
+/* ---- host memory: src/lunarscout/_numba_horizon/psr_cuda.py:234-238
+ *      (allocate_pinned_horizon_buffer) ---- */
+/* Page-locked host memory for H2D/D2H staging (cudaHostAlloc). */
+ls200_status ls200_host_alloc(int64_t bytes, void **out);
+ls200_status ls200_host_free(void *ptr);
+
+/* FP32 FMA issue-rate probe (TFLOP/s, 2 flops per FMA) on this device: the
+ * measured denominator of the march's FP32 roofline.  No reference
+ * counterpart. */
+ls200_status ls200_fp32_probe(ls200_context *ctx, int iterations, double *tflops);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* LS200_H */

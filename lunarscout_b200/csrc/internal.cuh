@@ -1,0 +1,156 @@
+// Internal declarations shared by the ls200 translation units.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <cstdio>
+#include <cstring>
+#include <mutex>
+#include <stdexcept>
+#include <string>
+
+#include "../../include/ls200.h"
+
+namespace ls200 {
+
+constexpr int kMaxLevels = 20;   // 4^19 cells per side is far beyond any DEM
+constexpr int kSegmentFields = 18;
+constexpr int kMarchFields = 16;  // fields 0,1,4..17 of a segment
+
+// An error carrying the status it maps to at the C boundary.
+struct Error : std::runtime_error {
+    ls200_status status;
+    Error(ls200_status s, const std::string &message) : std::runtime_error(message), status(s) {}
+};
+
+void set_last_error(const std::string &message);
+
+#define LS_CUDA(call)                                                                  \
+    do {                                                                               \
+        cudaError_t e_ = (call);                                                       \
+        if (e_ != cudaSuccess) {                                                       \
+            throw ::ls200::Error(LS200_ERR_CUDA, std::string(#call) + ": " +           \
+                                                     cudaGetErrorString(e_));          \
+        }                                                                              \
+    } while (0)
+
+#define LS_REQUIRE(cond, message)                                                      \
+    do {                                                                               \
+        if (!(cond)) throw ::ls200::Error(LS200_ERR_INVALID, (message));               \
+    } while (0)
+
+// Run `body` and translate exceptions into a status + thread-local message.
+template <class F>
+ls200_status guard(F &&body) {
+    try {
+        body();
+        return LS200_OK;
+    } catch (const Error &e) {
+        set_last_error(e.what());
+        return e.status;
+    } catch (const std::bad_alloc &) {
+        set_last_error("host allocation failed");
+        return LS200_ERR_CUDA;
+    } catch (const std::exception &e) {
+        set_last_error(e.what());
+        return LS200_ERR_CUDA;
+    } catch (...) {
+        set_last_error("unknown failure");
+        return LS200_ERR_CUDA;
+    }
+}
+
+// A growable device buffer owned by a context.
+struct DeviceBuffer {
+    void *ptr = nullptr;
+    size_t bytes = 0;
+    void reserve(size_t n) {
+        if (n <= bytes) return;
+        if (ptr) cudaFree(ptr);
+        ptr = nullptr;
+        bytes = 0;
+        LS_CUDA(cudaMalloc(&ptr, n));
+        bytes = n;
+    }
+    template <class T>
+    T *as() const { return static_cast<T *>(ptr); }
+    ~DeviceBuffer() {
+        if (ptr) cudaFree(ptr);
+    }
+};
+
+struct PyramidLevel {
+    int offset, width, height;
+};
+
+}  // namespace ls200
+
+struct ls200_dem {
+    ls200_context *ctx = nullptr;
+    int width = 0, height = 0;
+    int level_count = 0;
+    int64_t mip_count = 0;
+    ls200::PyramidLevel levels[ls200::kMaxLevels];
+    float *level0 = nullptr;  // device [height, width]
+    float *mips = nullptr;    // device [mip_count]
+    double geo_transform[6];
+    double projection[6];
+    float map_parameters[11];
+};
+
+struct ls200_context {
+    int device = 0;
+    cudaStream_t own_stream = nullptr;
+    cudaStream_t stream = nullptr;
+    std::mutex lock;
+    cudaDeviceProp props{};
+    ls200::DeviceBuffer segments;   // [A, C, D, 18]
+    ls200::DeviceBuffer slopes;     // az-major working slopes [A, P]
+    ls200::DeviceBuffer output;     // pixel-major [P, A]
+    ls200::DeviceBuffer scratch;
+    ls200::DeviceBuffer counters;   // 3 x u64: node visits, level-0 samples, ray steps
+    bool counting = false;
+    uint64_t last_visits = 0, last_samples = 0, last_steps = 0;
+    cudaEvent_t events[ls200::kMaxLevels + 2] = {};
+};
+
+namespace ls200 {
+
+// Make the context's device current on this thread.
+void activate(ls200_context *ctx);
+
+int pyramid_layout(int width, int height, PyramidLevel *levels, int capacity,
+                   int64_t *mip_count);
+
+// Build all mip levels of `dem` on ctx->stream from dem->level0.
+void build_pyramid_device(ls200_context *ctx, ls200_dem *dem);
+
+// Segment generation into device memory.
+void segments_device(ls200_context *ctx, ls200_dem *const *dems, int dem_count,
+                     int tile_column, int tile_row, int tile_width, int azimuth_count,
+                     double maximum_distance_m, double observer_elevation_m, int subpatch,
+                     float *device_segments);
+
+struct MarchTile {
+    const float *segments;  // device [A, C, D, 18]
+    int azimuth_count, center_count, dem_count;
+    int tile_column, tile_row, tile_width, tile_height, subpatch;
+    float observer_elevation;
+};
+
+// One pass into the az-major working buffer slopes[A, P]; first_pass starts
+// every ray at -inf without reading `slopes`.
+void march_pass_device(ls200_context *ctx, const MarchTile &tile, const ls200_dem *primary,
+                       const ls200_dem *active, int pass_index, bool first_pass,
+                       float *slopes_az_major);
+
+// az-major [A, P] -> pixel-major [P, A], optionally as degrees.
+void transpose_slopes(ls200_context *ctx, const float *az_major, int azimuth_count,
+                      int pixel_count, float *pixel_major, bool degrees);
+void pixel_major_to_az_major(ls200_context *ctx, const float *pixel_major, int azimuth_count,
+                             int pixel_count, float *az_major);
+void slopes_to_degrees_device(ls200_context *ctx, const float *slopes, int64_t count,
+                              float *degrees);
+
+}  // namespace ls200

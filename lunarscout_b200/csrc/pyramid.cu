@@ -1,0 +1,59 @@
+// Factor-four maximum-elevation pyramid (pyramid.py:19-31,110-138;
+// cuda_backend.py:134-153).  Each mip cell holds the maximum valid elevation
+// (finite and > -20000) of its 4x4 block of the level below, or -32000 when
+// the block has no valid cell.  One launch per level, all on the context
+// stream with no host round trip between levels.
+#include "internal.cuh"
+
+namespace ls200 {
+
+__device__ __forceinline__ bool valid_elevation(float v) {
+    return !isnan(v) && !isinf(v) && v > -20000.0f;
+}
+
+// One thread per destination cell; a warp covers 32 adjacent destination
+// columns, i.e. 128 contiguous source floats on each of the 4 source rows.
+__global__ void __launch_bounds__(256) pyramid_downsample(const float *__restrict__ source,
+                                                          int source_width, int source_height,
+                                                          float *__restrict__ destination,
+                                                          int width, int height) {
+    const int x = blockIdx.x * blockDim.x + threadIdx.x;
+    const int y = blockIdx.y * blockDim.y + threadIdx.y;
+    if (x >= width || y >= height) return;
+    float best = -32000.0f;
+    const int x0 = x * 4, y0 = y * 4;
+#pragma unroll
+    for (int dy = 0; dy < 4; ++dy) {
+        const int yy = y0 + dy;
+        if (yy >= source_height) break;
+        const float *row = source + static_cast<size_t>(yy) * source_width;
+#pragma unroll
+        for (int dx = 0; dx < 4; ++dx) {
+            const int xx = x0 + dx;
+            if (xx < source_width) {
+                const float v = __ldg(row + xx);
+                if (valid_elevation(v) && v > best) best = v;
+            }
+        }
+    }
+    destination[static_cast<size_t>(y) * width + x] = best;
+}
+
+void build_pyramid_device(ls200_context *ctx, ls200_dem *dem) {
+    const float *source = dem->level0;
+    int sw = dem->width, sh = dem->height;
+    for (int level = 1; level < dem->level_count; ++level) {
+        const PyramidLevel &L = dem->levels[level];
+        float *destination = dem->mips + L.offset;
+        dim3 block(32, 8);
+        dim3 grid((L.width + block.x - 1) / block.x, (L.height + block.y - 1) / block.y);
+        pyramid_downsample<<<grid, block, 0, ctx->stream>>>(source, sw, sh, destination,
+                                                            L.width, L.height);
+        LS_CUDA(cudaGetLastError());
+        source = destination;
+        sw = L.width;
+        sh = L.height;
+    }
+}
+
+}  // namespace ls200

@@ -140,6 +140,15 @@ def _declare(library: ctypes.CDLL) -> None:
 _EXTRA_DECLARATIONS: list = []
 
 
+def _declare_extra(name: str, argtypes: list, restype) -> None:
+    """Register a ctypes signature from a submodule (applied on load)."""
+    _EXTRA_DECLARATIONS.append((name, argtypes, restype))
+    if _LIB is not None and hasattr(_LIB, name):
+        function = getattr(_LIB, name)
+        function.argtypes = argtypes
+        function.restype = restype
+
+
 def default_threads() -> int:
     return max(1, len(os.sched_getaffinity(0)))
 

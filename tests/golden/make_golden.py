@@ -1,0 +1,281 @@
+"""Generate the committed golden fixtures under tests/golden/.
+
+Run in a container that has the reference checkout (read-only) at
+REFERENCE_ROOT; the GPU box never runs this.  It imports the reference's own
+Python modules through a stub package (its top-level ``__init__`` needs
+pyproj/rasterio, absent here) and extracts:
+
+* horizon_production.npz — the reference's single-pixel two-DEM production
+  fixture (tests/data/numba_horizon/phase1_reference_rays.npz) with the
+  segment tensor the reference's own tests feed it
+  (geometry.build_subpatch_segments), the C# golden per-DEM and final slopes
+  and the 932-row C# traversal trace (phase4d_production_segments.json), the
+  C# bilinear-boundary trace, and the output of the reference's production
+  Numba kernel (cuda_backend.subpatch_hierarchy_kernel) executed by Numba's
+  CUDA simulator on CPU.
+* pyramids.npz — C# pyramid captures incl. the NaN/inf/-20000 fixture.
+* segments_halo.npz — the 16x16-tile, 16-azimuth, two-DEM halo fixture: the
+  C# segment tensor, the reference's Numba segment tensor and its DEMs.
+
+Usage: python tests/golden/make_golden.py [--simulate]
+(--simulate re-runs the simulator capture, ~5 min).
+"""
+
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import sys
+import types
+from fractions import Fraction
+from pathlib import Path
+
+import numpy as np
+
+REFERENCE_ROOT = Path(os.environ.get("LUNARSCOUT_REFERENCE", "/root/reference"))
+PACKAGE = REFERENCE_ROOT / "src" / "lunarscout"
+DATA = REFERENCE_ROOT / "tests" / "data" / "numba_horizon"
+OUT = Path(__file__).resolve().parent
+
+
+def import_reference():
+    os.environ.setdefault("NUMBA_CACHE_DIR", "/tmp/lunarscout-numba-cache")
+    sys.dont_write_bytecode = True
+    if "lunarscout" not in sys.modules:
+        stub = types.ModuleType("lunarscout")
+        stub.__path__ = [str(PACKAGE)]
+        sys.modules["lunarscout"] = stub
+
+
+def _artifact():
+    from lunarscout._numba_horizon.contract import load_reference_artifact
+
+    return load_reference_artifact(DATA / "phase1_reference_rays.json",
+                                   DATA / "phase1_reference_rays.npz")
+
+
+def _dem(artifact, prefix):
+    from lunarscout._numba_horizon.geometry import DemGrid, ProjectionParameters
+
+    return DemGrid(
+        artifact.arrays[f"{prefix}__elevation_m"],
+        artifact.arrays[f"{prefix}__geo_transform"],
+        ProjectionParameters.from_array(artifact.arrays[f"{prefix}__pyramid__projection_parameters"]),
+    )
+
+
+def _pyramid_dict(artifact, prefix, name):
+    from lunarscout._numba_horizon.contract import PyramidArrays
+
+    p = PyramidArrays.from_artifact(artifact.arrays, f"{prefix}__pyramid")
+    return {
+        f"{name}_level0": p.level0,
+        f"{name}_mips": p.mips,
+        f"{name}_levels": p.levels,
+        f"{name}_map": p.map_parameters,
+        f"{name}_projection": p.projection_parameters,
+    }
+
+
+TRACE_FIELDS = ("s_km", "true_distance_m", "level", "cell_x", "cell_y", "pixel_x",
+                "pixel_y", "maximum_elevation_m", "sample_elevation_m", "sample_slope",
+                "advance_km", "action")
+
+
+def _trace(capture):
+    return np.asarray([[np.nan if row[f] is None else row[f] for f in TRACE_FIELDS]
+                       for row in capture["trace"]], dtype=np.float32)
+
+
+def _exact_fmaf(a, b, c):
+    """Correctly rounded float32 fma (Numba's simulator has no libdevice)."""
+    a, b, c = np.float32(a), np.float32(b), np.float32(c)
+    exact = Fraction(float(a)) * Fraction(float(b)) + Fraction(float(c))
+    r = np.float32(float(exact))
+    best = None
+    for cand in (np.nextafter(r, np.float32(-np.inf)), r, np.nextafter(r, np.float32(np.inf))):
+        if not np.isfinite(cand):
+            continue
+        d = abs(Fraction(float(cand)) - exact)
+        if best is None or d < best[0] or (d == best[0] and int(cand.view(np.uint32)) & 1 == 0):
+            best = (d, cand)
+    return best[1]
+
+
+def simulate_reference_kernel(segments, pyramids):
+    """Run the reference's production kernel under Numba's CUDA simulator."""
+    os.environ["NUMBA_ENABLE_CUDASIM"] = "1"
+    from types import SimpleNamespace
+
+    import numba
+    import numba.cuda.libdevice as libdevice
+    from numba import cuda
+    from numba.cuda.simulator import kernel as simkernel
+
+    libdevice.fmaf = _exact_fmaf
+
+    class CudaProxy:
+        """Resolve cuda.* inside simulated kernels through the kernel context
+        (the reference binds ``cuda`` as a closure, not a global)."""
+
+        def __getattr__(self, name):
+            context = simkernel._get_kernel_context()
+            if context is not None and hasattr(context, name):
+                return getattr(context, name)
+            return getattr(cuda, name)
+
+    original_jit = cuda.jit
+
+    def jit(*args, **kwargs):
+        kwargs.pop("max_registers", None)
+        kwargs.pop("cache", None)
+        return original_jit(*args, **kwargs)
+
+    cuda.jit = jit
+    cuda.get_current_device = lambda: SimpleNamespace(name=b"simulator",
+                                                      compute_capability=(0, 0))
+    import lunarscout._cuda_runtime as runtime
+
+    runtime.import_numba_cuda = lambda: (numba, CudaProxy())
+    from lunarscout._numba_horizon.cuda_backend import CudaSession
+
+    session = CudaSession()
+    common = dict(tile_column=20, tile_row=20, tile_width=1, tile_height=1, subpatch_size=8)
+    pass0 = session.subpatch_hierarchical_pass(segments, pyramids[0], pyramids[0],
+                                               pass_index=0, **common)
+    final = session.subpatch_hierarchical_pass(segments, pyramids[0], pyramids[1],
+                                               pass_index=1, slopes=pass0, **common)
+    return pass0.reshape(-1), final.reshape(-1)
+
+
+def horizon_production(simulate: bool) -> None:
+    from lunarscout._numba_horizon.geometry import (
+        GridConvergenceInput, build_subpatch_segments)
+    from lunarscout._numba_horizon.contract import PyramidArrays
+
+    artifact = _artifact()
+    base = "single_pixel_multi_dem_production__horizon_buffer_fixture"
+    dems = [_dem(artifact, f"{base}__dem_{i}") for i in range(2)]
+    pyramids = [PyramidArrays.from_artifact(artifact.arrays, f"{base}__dem_{i}__pyramid")
+                for i in range(2)]
+    segments, _, _ = build_subpatch_segments(
+        dems, tile_column=20, tile_row=20, tile_width=1, azimuth_count=1440,
+        maximum_distance_m=1_000_000, observer_elevation_m=0, subpatch_size=8,
+        grid_convergence=GridConvergenceInput(0.0, 0.0, 0.0))
+    capture = json.loads((DATA / "phase4d_production_segments.json").read_text())
+    production = capture["production_hierarchy_case"]
+    boundary = capture["bilinear_boundary_case"]
+    arrays = {
+        "segments": segments.astype(np.float32),
+        "csharp_per_dem_slopes": np.asarray(production["per_dem_slopes"], np.float32).reshape(2, 1440),
+        "csharp_final_slopes": np.asarray(production["final_slopes"], np.float32),
+        "csharp_final_degrees": np.asarray(production["final_degrees"], np.float32),
+        "csharp_trace": _trace(production),
+        "csharp_trace_segments": np.asarray(capture["segments"], np.float32),
+        "csharp_trace_observer_z": np.float32(dems[0].elevation(20, 20)),
+        "csharp_trace_maximum_slope": np.float32(production["csharp_hierarchy_maximum_slope"]),
+        "boundary_segments": np.asarray(boundary["segments"], np.float32),
+        "boundary_trace": _trace(boundary),
+        "boundary_maximum_slope": np.float32(boundary["csharp_hierarchy_maximum_slope"]),
+    }
+    for i in range(2):
+        arrays[f"dem{i}_geo_transform"] = dems[i].geo_transform
+        arrays.update(_pyramid_dict(artifact, f"{base}__dem_{i}", f"dem{i}"))
+    # The boundary case DEM (single_obstacle_north), its observer and resolution.
+    case = next(c for c in artifact.metadata["cases"] if c["id"] == "single_obstacle_north")
+    bdem = _dem(artifact, "single_obstacle_north__dem_0")
+    arrays["boundary_elevation"] = bdem.elevation_m
+    observer = case["observer"]
+    arrays["boundary_observer_z"] = np.float32(
+        float(bdem.elevation(observer["pixel_x"], observer["pixel_y"])) + float(observer["elevation_m"]))
+    arrays["boundary_radius"] = np.float32(bdem.projection.radius_m)
+    arrays["boundary_resolution"] = np.float32(case["ray_fit_passes"][0]["map_resolution_m"])
+    target = OUT / "horizon_production.npz"
+    if simulate or not target.exists():
+        pass0, final = simulate_reference_kernel(segments, pyramids)
+    else:
+        with np.load(target) as old:
+            pass0, final = old["reference_sim_pass0"], old["reference_sim_final"]
+    arrays["reference_sim_pass0"] = pass0
+    arrays["reference_sim_final"] = final
+    np.savez_compressed(target, **arrays)
+
+
+def pyramids_fixture() -> None:
+    artifact = _artifact()
+    arrays = {}
+    names = []
+    for case in artifact.metadata["cases"]:
+        for pyramid in case["pyramids"]:
+            prefix = f"{case['id']}__dem_{pyramid['dem_index']}__pyramid"
+            levels = artifact.arrays[f"{prefix}__level_metadata"]
+            if levels[0, 2] * levels[0, 3] > 5000:
+                continue
+            name = f"p{len(names)}"
+            names.append(prefix)
+            arrays[f"{name}_levels"] = levels
+            for level in range(len(levels)):
+                arrays[f"{name}_level{level}"] = artifact.arrays[f"{prefix}__level_{level}"]
+    fixture = "invalid_values_odd_dimensions__pyramid_fixture"
+    arrays["invalid_elevation"] = artifact.arrays[f"{fixture}__elevation_m"]
+    arrays["invalid_levels"] = artifact.arrays[f"{fixture}__level_metadata"]
+    for level in range(3):
+        arrays[f"invalid_level{level}"] = artifact.arrays[f"{fixture}__level_{level}"]
+    arrays["names"] = np.array(names)
+    np.savez_compressed(OUT / "pyramids.npz", **arrays)
+
+
+def segments_halo() -> None:
+    from lunarscout._numba_horizon.geometry import (
+        GridConvergenceInput, build_subpatch_segments_numba)
+
+    artifact = _artifact()
+    fixture = next(f for f in artifact.metadata["subpatch_fixtures"]
+                   if f["id"] == "boundary_halo_multi_dem_16az")
+    config = fixture["configuration"]
+    dems = [_dem(artifact, f"multi_dem_outer_obstacle_east__dem_{i}") for i in range(2)]
+    kwargs = dict(tile_column=config["tile_column"], tile_row=config["tile_row"],
+                  tile_width=config["tile_width"], azimuth_count=config["azimuth_count"],
+                  maximum_distance_m=config["max_distance_m"],
+                  observer_elevation_m=config["observer_elevation_m"],
+                  subpatch_size=config["subpatch_size"])
+    numba_segments, _, _ = build_subpatch_segments_numba(
+        dems, grid_convergence=GridConvergenceInput(0.0, 0.0, 0.0), parallel=False, **kwargs)
+    arrays = {
+        "csharp_segments": artifact.arrays["boundary_halo_multi_dem_16az__subpatch_fixture__segment_values"],
+        "reference_numba_segments": numba_segments,
+        "config": np.array([config["tile_column"], config["tile_row"], config["tile_width"],
+                            config["tile_height"], config["subpatch_size"],
+                            config["azimuth_count"], config["max_distance_m"]], dtype=np.int64),
+    }
+    for i, dem in enumerate(dems):
+        arrays[f"dem{i}_elevation"] = dem.elevation_m
+        arrays[f"dem{i}_geo_transform"] = dem.geo_transform
+        arrays[f"dem{i}_projection"] = np.array(
+            (dem.projection.radius_m, dem.projection.latitude_origin_rad,
+             dem.projection.longitude_origin_rad, dem.projection.scale,
+             dem.projection.false_easting_m, dem.projection.false_northing_m), np.float64)
+    np.savez_compressed(OUT / "segments_halo.npz", **arrays)
+
+
+def main() -> None:
+    parser = argparse.ArgumentParser()
+    parser.add_argument("--simulate", action="store_true")
+    parser.add_argument("--only", default="")
+    args = parser.parse_args()
+    import_reference()
+    jobs = {
+        "horizon": lambda: horizon_production(args.simulate),
+        "pyramids": pyramids_fixture,
+        "segments": segments_halo,
+    }
+    for name, job in jobs.items():
+        if args.only and name not in args.only.split(","):
+            continue
+        job()
+        print("wrote", name)
+
+
+if __name__ == "__main__":
+    main()

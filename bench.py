@@ -393,6 +393,33 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
+def run_profile_case():
+    """One site-scale tile marched twice (launches 3-4 are the second step's
+    two passes); used under ncu, never timed."""
+    import torch
+    from lunarscout_b200.cuda_backend import CudaSession
+
+    primary, regional = build_dems()
+    session = CudaSession(0)
+    dems = [session.upload_dem_grid(primary), session.upload_dem_grid(regional)]
+    (tile_row, tile_column), = tile_schedule(0, 1, 1)
+    centers = (TILE // 8 + 2) ** 2
+    segments = torch.empty((AZIMUTHS, centers, 2, 18), dtype=torch.float32, device="cuda")
+    output = torch.empty((TILE * TILE, AZIMUTHS), dtype=torch.float32, device="cuda")
+    session.generate_segments_device(dems, segments.data_ptr(), tile_column=tile_column,
+                                     tile_row=tile_row, azimuth_count=AZIMUTHS,
+                                     maximum_distance_m=RANGE_M,
+                                     observer_elevation_m=OBSERVER_M)
+    for _ in range(2):
+        session.march_all_passes_device(segments.data_ptr(), AZIMUTHS, centers, dems,
+                                        tile_column=tile_column, tile_row=tile_row,
+                                        observer_elevation_m=OBSERVER_M,
+                                        device_out=output.data_ptr())
+    session.synchronize()
+    session.close()
+    log("[bench] profile case done")
+
+
 def main():
     parser = argparse.ArgumentParser()
     parser.add_argument("--gpus", type=int, default=1)
@@ -402,10 +429,14 @@ def main():
     parser.add_argument("--cpu-seconds", type=float, default=12.0)
     parser.add_argument("--reference-seconds", type=float, default=8.0)
     parser.add_argument("--skip-cpu", action="store_true")
+    parser.add_argument("--profile", action="store_true",
+                        help="small profiling case: one tile, two march steps, no timing")
     args = parser.parse_args()
     if args.warmup < 3:
         args.warmup = 3
-    if args.impl == "reference":
+    if args.profile:
+        run_profile_case()
+    elif args.impl == "reference":
         run_reference(args)
     else:
         run_ours(args)

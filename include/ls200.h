@@ -68,6 +68,8 @@ ls200_status ls200_dem_create(ls200_context *ctx, const float *level0, int width
                               const float *mips, const double *geo_transform,
                               const double *projection, const float *map_parameters,
                               ls200_dem **out);
+/* A DEM must be destroyed before its context; ls200_context_destroy releases
+ * the DEMs still alive, after which their handles are invalid. */
 ls200_status ls200_dem_destroy(ls200_dem *dem);
 /* Copies the device mips back (e.g. to write a .pyr.bin cache). */
 ls200_status ls200_dem_download_mips(ls200_dem *dem, float *mips, int64_t capacity);

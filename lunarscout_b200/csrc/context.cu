@@ -88,6 +88,13 @@ ls200_status ls200_context_destroy(ls200_context *ctx) {
         if (!ctx) return;
         cudaSetDevice(ctx->device);
         cudaStreamSynchronize(ctx->stream);
+        // DEMs still alive belong to this context: release them with it.
+        for (ls200_dem *dem : ctx->dems) {
+            if (dem->level0) cudaFree(dem->level0);
+            if (dem->mips) cudaFree(dem->mips);
+            delete dem;
+        }
+        ctx->dems.clear();
         for (auto &event : ctx->events)
             if (event) cudaEventDestroy(event);
         if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
@@ -182,6 +189,7 @@ ls200_status ls200_dem_create(ls200_context *ctx, const float *level0, int width
                 build_pyramid_device(ctx, dem);
             }
             LS_CUDA(cudaStreamSynchronize(ctx->stream));
+            ctx->dems.insert(dem);
         } catch (...) {
             if (dem->level0) cudaFree(dem->level0);
             if (dem->mips) cudaFree(dem->mips);
@@ -198,6 +206,7 @@ ls200_status ls200_dem_destroy(ls200_dem *dem) {
         std::lock_guard<std::mutex> hold(dem->ctx->lock);
         activate(dem->ctx);
         cudaStreamSynchronize(dem->ctx->stream);
+        dem->ctx->dems.erase(dem);
         if (dem->level0) cudaFree(dem->level0);
         if (dem->mips) cudaFree(dem->mips);
         delete dem;

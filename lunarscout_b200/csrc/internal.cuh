@@ -7,6 +7,7 @@
 #include <cstdio>
 #include <cstring>
 #include <mutex>
+#include <set>
 #include <stdexcept>
 #include <string>
 
@@ -113,6 +114,7 @@ struct ls200_context {
     bool counting = false;
     uint64_t last_visits = 0, last_samples = 0, last_steps = 0;
     cudaEvent_t events[ls200::kMaxLevels + 2] = {};
+    std::set<ls200_dem *> dems;  // live DEMs, released with the context
 };
 
 namespace ls200 {

@@ -124,6 +124,48 @@ __device__ __forceinline__ float bound_slope(float dist, float height, float rad
     return __fdiv_rn(local_z, local_x);
 }
 
+// Exactly `possible <= current` for the four-cell bound `possible` of the
+// reference (near field: fl((h - oz) / tn); far field: bound_slope), at a
+// fraction of its cost.  The cull test is the most frequent operation of the
+// march and `possible` only feeds this comparison, so an approximation may
+// decide it whenever it lies outside a guard band around `current`:
+//   near: __fdividef has at most 2 ulp error;
+//   far:  the numerator is the exact one; z = num * rcp(den) is within 3 ulp
+//         of fl(num / den); with local_x^2 > tn^2 / 4 (bound below 60 deg)
+//         the cancellation in local_x^2 amplifies that by at most 3, and
+//         rsqrtf adds 2 ulp: the approximation is within 2e-6 (relative) of
+//         the exact FP32 value.
+// The band is 1e-5 relative, five times that bound; inside it, and for
+// steeper bounds, the exact arithmetic of the reference decides.
+__device__ __forceinline__ bool bound_culled(bool near, float true_near, float height,
+                                             float radius, float observer_z,
+                                             float observer_radius, float inverse_denominator,
+                                             float current) {
+    float approx;
+    if (near) {
+        approx = __fdividef(__fsub_rn(height, observer_z), true_near);
+    } else {
+        const float squared = __fmul_rn(true_near, true_near);
+        const float height_delta = __fsub_rn(height, observer_z);
+        float radius_sum = __fadd_rn(__fmul_rn(2.0f, radius), height);
+        radius_sum = __fadd_rn(radius_sum, observer_z);
+        const float numerator = __fmaf_rn(height_delta, radius_sum, -squared);
+        const float local_z = __fmul_rn(numerator, inverse_denominator);
+        const float lx2 = __fmaf_rn(true_near, true_near, -__fmul_rn(local_z, local_z));
+        if (!(lx2 > 0.25f * squared)) {
+            return bound_slope(true_near, height, radius, observer_z, observer_radius) <= current;
+        }
+        approx = __fmul_rn(local_z, rsqrtf(lx2));
+    }
+    const float band = 1e-5f * fmaxf(fabsf(approx), fabsf(current));
+    if (approx < current - band) return true;
+    if (approx > current + band) return false;
+    const float possible =
+        near ? __fdiv_rn(__fsub_rn(height, observer_z), true_near)
+             : bound_slope(true_near, height, radius, observer_z, observer_radius);
+    return possible <= current;
+}
+
 __device__ __forceinline__ int clamp_center(int requested, int dem_size, int subpatch) {
     const int half = subpatch / 2;
     int maximum = dem_size - half;
@@ -225,6 +267,7 @@ __global__ void __launch_bounds__(128) march_pass_kernel(const __grid_constant__
     const float resolution = __fmul_rn(__fadd_rn(column_res, row_res), 0.5f);
     const float radius = P.radius;
     const float observer_radius = __fadd_rn(radius, observer_z);
+    const float inverse_denominator = __frcp_rn(__fmul_rn(2.0f, observer_radius));
 
     // ---- hierarchy_maximum (cuda_backend.py:656-874) ----
     float current = -1e30f;
@@ -329,11 +372,8 @@ __global__ void __launch_bounds__(128) march_pass_kernel(const __grid_constant__
             }
             float true_near = __fmaf_rn(-scale_f, resolution, true_m);
             true_near = true_near > 1.0f ? true_near : 1.0f;
-            const float possible =
-                s < 0.5f ? __fdiv_rn(__fsub_rn(maximum_height, observer_z), true_near)
-                         : bound_slope(true_near, maximum_height, radius, observer_z,
-                                       observer_radius);
-            if (possible <= current) {
+            if (bound_culled(s < 0.5f, true_near, maximum_height, radius, observer_z,
+                             observer_radius, inverse_denominator, current)) {
                 s = __fadd_rn(s, skip);
                 break;
             }

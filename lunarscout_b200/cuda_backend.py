@@ -14,6 +14,7 @@ from __future__ import annotations
 import ctypes
 import threading
 import time
+import weakref
 from dataclasses import dataclass
 
 import numpy as np
@@ -42,9 +43,10 @@ class DeviceDem:
         self.height = height
 
     def close(self) -> None:
-        if self.handle:
+        # The context releases its DEMs itself; only an open session frees one.
+        if self.handle and self._session._ctx:
             library().ls200_dem_destroy(self.handle)
-            self.handle = ctypes.c_void_p(None)
+        self.handle = ctypes.c_void_p(None)
 
     def __del__(self):  # pragma: no cover - best effort release
         try:
@@ -82,6 +84,7 @@ class CudaSession:
         self.info = CudaDeviceInfo(name.value.decode(), (major.value, minor.value))
         self.sm_count = sms.value
         self._lock = threading.Lock()
+        self._dems = weakref.WeakSet()
         self._production_pyramids = None
         self._production_device_dems = None
         self._production_timings = threading.local()
@@ -89,9 +92,8 @@ class CudaSession:
     # -- lifecycle ---------------------------------------------------------
     def close(self) -> None:
         if getattr(self, "_ctx", None):
-            if self._production_device_dems:
-                for dem in self._production_device_dems:
-                    dem.close()
+            for dem in list(self._dems):
+                dem.close()
             library().ls200_context_destroy(self._ctx)
             self._ctx = None
 
@@ -136,7 +138,9 @@ class CudaSession:
             mips_ptr = mips.ctypes.data
         call("ls200_dem_create", self._ctx, level0, width, height, mips_ptr, geo, proj, mp,
              ctypes.byref(handle))
-        return DeviceDem(self, handle.value, width, height)
+        dem = DeviceDem(self, handle.value, width, height)
+        self._dems.add(dem)
+        return dem
 
     def upload_pyramid(self, pyramid) -> DeviceDem:
         geo, proj, mp = _pyramid_geo(pyramid)

@@ -128,6 +128,45 @@ ls200_status ls200_last_counters(ls200_context *ctx, int64_t *visits, int64_t *s
 ls200_status ls200_slopes_to_degrees(ls200_context *ctx, const float *slopes, int64_t count,
                                      float *degrees);
 
+/* ---- lighting products: src/lunarscout/_numba_horizon/lightmap_cuda.py:187-276
+ *      (LightmapCudaSession) and psr_cuda.py:191-375 (PsrCudaSession) ---- */
+typedef struct ls200_vectors ls200_vectors;
+/* Device-resident float32 Moon-ME vectors [count, 3] (metres); the sessions
+ * keep one resident per vector set (lightmap_cuda.py:238-242). */
+ls200_status ls200_vectors_create(ls200_context *ctx, const float *vectors, int count,
+                                  ls200_vectors **out);
+ls200_status ls200_vectors_destroy(ls200_vectors *vectors);
+/* Stage one 128x128 patch: patch_dem float32[128*128] (zero outside the valid
+ * rect), horizons float32[128*128*1440] degrees, the DEM's geotransform and
+ * projection (6 f64 each) and the patch window. */
+ls200_status ls200_lighting_load(ls200_context *ctx, const float *patch_dem,
+                                 const double *geo_transform, const double *projection,
+                                 const float *horizons, int tile_x, int tile_y,
+                                 int valid_width, int valid_height);
+/* Times [time_start, time_start+time_count) of the staged patch into host
+ * `out` [time_count, 128, 128]: signal 0 = float32 sun fraction, 1 = uint8
+ * int(255*fraction), 2 = float32 body-centre margin (deg). */
+ls200_status ls200_lighting_run(ls200_context *ctx, const ls200_vectors *vectors,
+                                int time_start, int time_count, int signal, void *out);
+/* PSR byte mask (255 = permanently shadowed) of the staged patch over all
+ * vectors into host out[128*128]. */
+ls200_status ls200_psr_run(ls200_context *ctx, const ls200_vectors *vectors, uint8_t *out);
+/* Device-resident batch of up to 32 patches: device patch_dems
+ * [n,128,128], host geo_transforms/projections [n,6] f64, host windows
+ * [n,4] (tile_x, tile_y, valid_width, valid_height), device horizons
+ * [n,128,128,1440], device frames scratch [n,16384,12] f32, device out
+ * [n, time_count, 128*128] (PSR, signal 3: [n, 128*128] over all vectors). */
+ls200_status ls200_lighting_device(ls200_context *ctx, int tile_count, const float *patch_dems,
+                                   const double *geo_transforms, const double *projections,
+                                   const int32_t *windows, const float *horizons,
+                                   const ls200_vectors *vectors, int time_start,
+                                   int time_count, int signal, float *frames, void *out);
+/* Diagnostic: sun fraction at given (azimuth, elevation) in degrees for n
+ * horizon rows float32[n,1440] (lightmap.py:32-73). */
+ls200_status ls200_sun_fraction(ls200_context *ctx, const float *horizons,
+                                const float *azimuth_deg, const float *elevation_deg, int n,
+                                float *out);
+
 /* ---- host memory: src/lunarscout/_numba_horizon/psr_cuda.py:234-238
  *      (allocate_pinned_horizon_buffer) ---- */
 /* Page-locked host memory for H2D/D2H staging (cudaHostAlloc). */

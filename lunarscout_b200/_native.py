@@ -84,6 +84,13 @@ SIGNATURES: dict[str, list] = {
     "ls200_set_counting": [_vp, _i],
     "ls200_last_counters": [_vp, _vp, _vp, _vp],
     "ls200_slopes_to_degrees": [_vp, _f32p, _i64, _f32p],
+    "ls200_vectors_create": [_vp, _f32p, _i, _vp],
+    "ls200_vectors_destroy": [_vp],
+    "ls200_lighting_load": [_vp, _f32p, _f64p, _f64p, _f32p, _i, _i, _i, _i],
+    "ls200_lighting_run": [_vp, _vp, _i, _i, _i, _vp],
+    "ls200_psr_run": [_vp, _vp, _vp],
+    "ls200_lighting_device": [_vp, _i, _vp, _vp, _vp, _vp, _vp, _vp, _i, _i, _i, _vp, _vp],
+    "ls200_sun_fraction": [_vp, _f32p, _f32p, _f32p, _i, _f32p],
     "ls200_host_alloc": [_i64, _vp],
     "ls200_host_free": [_vp],
     "ls200_fp32_probe": [_vp, _i, _vp],

@@ -95,6 +95,7 @@ ls200_status ls200_context_destroy(ls200_context *ctx) {
             delete dem;
         }
         ctx->dems.clear();
+        release_lighting_state(ctx);
         for (auto &event : ctx->events)
             if (event) cudaEventDestroy(event);
         if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);

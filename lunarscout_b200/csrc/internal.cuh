@@ -85,6 +85,8 @@ struct PyramidLevel {
     int offset, width, height;
 };
 
+struct LightingState;  // lighting tile buffers of a context (lighting_api.cu)
+
 }  // namespace ls200
 
 struct ls200_dem {
@@ -115,12 +117,16 @@ struct ls200_context {
     uint64_t last_visits = 0, last_samples = 0, last_steps = 0;
     cudaEvent_t events[ls200::kMaxLevels + 2] = {};
     std::set<ls200_dem *> dems;  // live DEMs, released with the context
+    ls200::LightingState *lighting = nullptr;
 };
 
 namespace ls200 {
 
 // Make the context's device current on this thread.
 void activate(ls200_context *ctx);
+
+// Free the lighting buffers and vector tables owned by a context.
+void release_lighting_state(ls200_context *ctx);
 
 int pyramid_layout(int width, int height, PyramidLevel *levels, int capacity,
                    int64_t *mip_count);

@@ -1,0 +1,232 @@
+// Lighting products against 1440-azimuth horizon tiles on sm_100a:
+// sun fraction (float32 and byte), body-centre margin, PSR.
+//
+// Semantics follow src/lunarscout/_numba_horizon/lightmap_cpu.py:25-183 (the
+// per-pixel FP64 east/north/up frame, float32 per time step, 16-slice solar
+// disk of src/lunarscout/_numba_horizon/lightmap.py:15-29) and
+// psr_cuda.py:57-186 (PSR).  Arithmetic is the reference CPU backend's, op by
+// op (this file builds with --fmad=false); atan2f is CUDA's.
+//
+// Design: the per-pixel frame (FP64 trigonometry) is computed once per tile
+// into 12 floats per pixel; the time loop is split into chunks so that a
+// tile's 16384 pixels x T times fill all SMs; one thread owns one pixel of
+// one chunk and writes time-major rows [t, 128*128] (coalesced across the
+// warp).  Many tiles may share one launch (blockIdx.z).
+#define LS200_LIGHTING_KERNELS
+#include "internal.cuh"
+#include "lighting.cuh"
+
+namespace ls200 {
+
+static bool g_constants_ready[64] = {};
+
+void ensure_lighting_constants(ls200_context *ctx) {
+    if (g_constants_ready[ctx->device]) return;
+    // Half-chords of a 16-column disk of radius float32(0.27) deg
+    // (lightmap.py:19-25), rounded once to float32; the normaliser is twice
+    // their float32 running sum.
+    float hc[16];
+    float sum = 0.0f;
+    for (int i = 0; i < 16; ++i) {
+        const double x = 7.5 - i;
+        hc[i] = static_cast<float>(std::sqrt(64.0 - x * x) / 8.0 * static_cast<double>(0.27f));
+        sum = sum + hc[i];
+    }
+    const float max_photons = 2.0f * sum;
+    LS_CUDA(cudaMemcpyToSymbol(c_half_circle, hc, sizeof hc));
+    LS_CUDA(cudaMemcpyToSymbol(c_max_photons, &max_photons, sizeof max_photons));
+    g_constants_ready[ctx->device] = true;
+}
+
+// FP64 east/north/up frame of one DEM pixel (lightmap_cpu.py:51-103).
+__device__ Frame32 pixel_frame(const TileGeo &g, int column, int row, float height) {
+    const double *gt = g.gt, *proj = g.proj;
+    const double crs_x = gt[0] + gt[1] * column + gt[2] * row;
+    const double crs_y = gt[3] + gt[4] * column + gt[5] * row;
+    const double xp = crs_x - proj[4];
+    const double yp = crs_y - proj[5];
+    const double rho = sqrt(xp * xp + yp * yp);
+    double latitude, longitude;
+    if (rho <= 1e-12) {
+        longitude = proj[2];
+        latitude = proj[1];
+    } else {
+        const double c = 2.0 * atan2(rho, 2.0 * proj[3] * proj[0]);
+        double sin_c, cos_c, sin_o, cos_o;
+        sincos(c, &sin_c, &cos_c);
+        sincos(proj[1], &sin_o, &cos_o);
+        latitude = asin(cos_c * sin_o + yp * sin_c * cos_o / rho);
+        longitude = proj[2] + atan2(xp * sin_c, rho * cos_o * cos_c - yp * sin_o * sin_c);
+    }
+    const double radius = proj[0] + static_cast<double>(height);
+    double sin_lat, cos_lat, sin_lon, cos_lon;
+    sincos(latitude, &sin_lat, &cos_lat);
+    sincos(longitude, &sin_lon, &cos_lon);
+    const double moon_x = radius * cos_lat * cos_lon;
+    const double moon_y = radius * cos_lat * sin_lon;
+    const double moon_z = radius * sin_lat;
+    const double up_x = cos_lat * cos_lon, up_y = cos_lat * sin_lon, up_z = sin_lat;
+    const double east_x = -sin_lon, east_y = cos_lon;
+    const double north_x = -sin_lat * cos_lon, north_y = -sin_lat * sin_lon, north_z = cos_lat;
+    Frame32 f;
+    f.v[0] = static_cast<float>(east_x);   // r00
+    f.v[1] = static_cast<float>(north_x);  // r01
+    f.v[2] = static_cast<float>(up_x);     // r02
+    f.v[3] = static_cast<float>(east_y);   // r10
+    f.v[4] = static_cast<float>(north_y);  // r11
+    f.v[5] = static_cast<float>(up_y);     // r12
+    f.v[6] = 0.0f;                         // r20
+    f.v[7] = static_cast<float>(north_z);  // r21
+    f.v[8] = static_cast<float>(up_z);     // r22
+    f.v[9] = static_cast<float>(-(moon_x * east_x + moon_y * east_y));
+    f.v[10] = static_cast<float>(-(moon_x * north_x + moon_y * north_y + moon_z * north_z));
+    f.v[11] = static_cast<float>(-(moon_x * up_x + moon_y * up_y + moon_z * up_z));
+    return f;
+}
+
+__global__ void __launch_bounds__(128) frames_kernel(const __grid_constant__ LightingBatch B) {
+    const int tile = blockIdx.y;
+    const int index = blockIdx.x * blockDim.x + threadIdx.x;
+    if (index >= kPatch * kPatch) return;
+    const TileGeo &g = B.tiles[tile];
+    const int sample = index % kPatch, line = index / kPatch;
+    Frame32 f{};
+    if (sample < g.valid_width && line < g.valid_height)
+        f = pixel_frame(g, g.tile_x + sample, g.tile_y + line,
+                        B.patch_dem[static_cast<size_t>(tile) * kPatch * kPatch + index]);
+    float *dst = B.frames + (static_cast<size_t>(tile) * kPatch * kPatch + index) * 12;
+#pragma unroll
+    for (int k = 0; k < 12; ++k) dst[k] = f.v[k];
+}
+
+template <int kSignal>
+__global__ void __launch_bounds__(128) lighting_kernel(const __grid_constant__ LightingBatch B) {
+    const int tile = blockIdx.z;
+    const int index = blockIdx.x * blockDim.x + threadIdx.x;
+    if (index >= kPatch * kPatch) return;
+    const TileGeo &g = B.tiles[tile];
+    const int sample = index % kPatch, line = index / kPatch;
+    const int t0 = B.time_start + blockIdx.y * B.chunk;
+    const int t1 = min(t0 + B.chunk, B.time_start + B.time_count);
+    const size_t plane = static_cast<size_t>(kPatch) * kPatch;
+    const size_t tile_out = static_cast<size_t>(tile) * B.time_count * plane;
+    if (sample >= g.valid_width || line >= g.valid_height) {
+        for (int t = t0; t < t1; ++t) {
+            const size_t o = tile_out + static_cast<size_t>(t - B.time_start) * plane + index;
+            if (kSignal == kSignalBytes) static_cast<uint8_t *>(B.out)[o] = 0;
+            else static_cast<float *>(B.out)[o] = 0.0f;
+        }
+        return;
+    }
+    Frame32 f;
+    const float *src = B.frames + (static_cast<size_t>(tile) * plane + index) * 12;
+#pragma unroll
+    for (int k = 0; k < 12; ++k) f.v[k] = src[k];
+    const float *horizon = B.horizons + (static_cast<size_t>(tile) * plane + index) * kAzimuths;
+    for (int t = t0; t < t1; ++t) {
+        const float *v = B.vectors + 3 * static_cast<size_t>(t);
+        float azimuth_deg, elevation;
+        body_direction(f, __ldg(v), __ldg(v + 1), __ldg(v + 2), azimuth_deg, elevation);
+        const size_t o = tile_out + static_cast<size_t>(t - B.time_start) * plane + index;
+        if (kSignal == kSignalMargin) {
+            static_cast<float *>(B.out)[o] = horizon_margin(horizon, azimuth_deg, elevation);
+        } else {
+            const float visible = sun_fraction(horizon, azimuth_deg, elevation);
+            if (kSignal == kSignalBytes)
+                static_cast<uint8_t *>(B.out)[o] =
+                    static_cast<uint8_t>(static_cast<int>(__fmul_rn(255.0f, visible)));
+            else
+                static_cast<float *>(B.out)[o] = visible;
+        }
+    }
+}
+
+// PSR (psr_cuda.py:57-186): 255 unless a reduced vector's centre rises above
+// the interpolated horizon minus 0.545/2 deg; exits at the first such vector.
+__global__ void __launch_bounds__(128) psr_kernel(const __grid_constant__ LightingBatch B) {
+    const int tile = blockIdx.z;
+    const int index = blockIdx.x * blockDim.x + threadIdx.x;
+    if (index >= kPatch * kPatch) return;
+    const TileGeo &g = B.tiles[tile];
+    const int sample = index % kPatch, line = index / kPatch;
+    uint8_t *out = static_cast<uint8_t *>(B.out) + static_cast<size_t>(tile) * kPatch * kPatch;
+    if (sample >= g.valid_width || line >= g.valid_height) {
+        out[index] = 0;
+        return;
+    }
+    Frame32 f;
+    const float *src = B.frames + (static_cast<size_t>(tile) * kPatch * kPatch + index) * 12;
+#pragma unroll
+    for (int k = 0; k < 12; ++k) f.v[k] = src[k];
+    const float *horizon =
+        B.horizons + (static_cast<size_t>(tile) * kPatch * kPatch + index) * kAzimuths;
+    uint8_t is_psr = 255;
+    for (int t = 0; t < B.time_count; ++t) {
+        const float *v = B.vectors + 3 * static_cast<size_t>(t);
+        float azimuth_deg, elevation;
+        body_direction(f, __ldg(v), __ldg(v + 1), __ldg(v + 2), azimuth_deg, elevation);
+        float position = __fmul_rn(azimuth_deg, 4.0f);
+        if (position >= static_cast<float>(kAzimuths)) position = 0.0f;
+        const int lower = static_cast<int>(position);
+        const float fraction = __fsub_rn(position, static_cast<float>(lower));
+        const int upper = lower + 1 >= kAzimuths ? 0 : lower + 1;
+        const float h1 = __ldg(horizon + lower), h2 = __ldg(horizon + upper);
+        const float h = __fadd_rn(h1, __fmul_rn(fraction, __fsub_rn(h2, h1)));
+        if (__fsub_rn(elevation, h) > -0.2725f) {
+            is_psr = 0;
+            break;
+        }
+    }
+    out[index] = is_psr;
+}
+
+// Diagnostic: sun fraction for given (azimuth, elevation) per horizon row
+// (the reference's _sun_fraction_reference, lightmap.py:32-73).
+__global__ void sun_fraction_kernel(const float *horizons, const float *azimuth_deg,
+                                    const float *elevation_deg, int n, float *out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    out[i] = sun_fraction(horizons + static_cast<size_t>(i) * kAzimuths, azimuth_deg[i],
+                          elevation_deg[i]);
+}
+
+int lighting_chunk(ls200_context *ctx, int tiles, int time_count) {
+    // Enough (pixel-block x chunk x tile) blocks for ~8 waves of 128-thread
+    // blocks on every SM, chunks of at least 16 time steps.
+    const int blocks_per_chunk = (kPatch * kPatch / 128) * tiles;
+    const int want = ctx->props.multiProcessorCount * 16 * 8;
+    int chunks = std::max(1, want / std::max(1, blocks_per_chunk));
+    chunks = std::min(chunks, std::max(1, time_count / 16));
+    return (time_count + chunks - 1) / chunks;
+}
+
+void lighting_launch(ls200_context *ctx, LightingBatch &B, int tiles, int signal) {
+    ensure_lighting_constants(ctx);
+    dim3 grid_frames(kPatch * kPatch / 128, tiles);
+    frames_kernel<<<grid_frames, 128, 0, ctx->stream>>>(B);
+    LS_CUDA(cudaGetLastError());
+    if (signal == kSignalPsr) {
+        dim3 grid(kPatch * kPatch / 128, 1, tiles);
+        psr_kernel<<<grid, 128, 0, ctx->stream>>>(B);
+    } else {
+        B.chunk = lighting_chunk(ctx, tiles, B.time_count);
+        dim3 grid(kPatch * kPatch / 128, (B.time_count + B.chunk - 1) / B.chunk, tiles);
+        if (signal == kSignalFraction)
+            lighting_kernel<kSignalFraction><<<grid, 128, 0, ctx->stream>>>(B);
+        else if (signal == kSignalBytes)
+            lighting_kernel<kSignalBytes><<<grid, 128, 0, ctx->stream>>>(B);
+        else
+            lighting_kernel<kSignalMargin><<<grid, 128, 0, ctx->stream>>>(B);
+    }
+    LS_CUDA(cudaGetLastError());
+}
+
+void sun_fraction_launch(ls200_context *ctx, const float *horizons, const float *azimuth_deg,
+                         const float *elevation_deg, int n, float *out) {
+    ensure_lighting_constants(ctx);
+    sun_fraction_kernel<<<(n + 127) / 128, 128, 0, ctx->stream>>>(horizons, azimuth_deg,
+                                                                  elevation_deg, n, out);
+    LS_CUDA(cudaGetLastError());
+}
+
+}  // namespace ls200

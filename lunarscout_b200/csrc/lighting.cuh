@@ -1,0 +1,141 @@
+// Lighting kernels' shared types and per-sample device arithmetic (included
+// by lighting.cu and lighting_api.cu).  Arithmetic follows the reference CPU
+// backend (src/lunarscout/_numba_horizon/lightmap_cpu.py:105-183) operation by
+// operation; the translation units build with --fmad=false.
+#pragma once
+
+#include "internal.cuh"
+
+namespace ls200 {
+
+constexpr int kPatch = 128;
+constexpr int kAzimuths = 1440;
+constexpr int kMaxBatchTiles = 32;
+enum { kSignalFraction = 0, kSignalBytes = 1, kSignalMargin = 2, kSignalPsr = 3 };
+
+struct Frame32 {
+    float v[12];  // r00 r01 r02 r10 r11 r12 r20 r21 r22 tx ty tz
+};
+
+struct TileGeo {
+    double gt[6];
+    double proj[6];
+    int tile_x, tile_y, valid_width, valid_height;
+};
+
+struct LightingBatch {
+    TileGeo tiles[kMaxBatchTiles];
+    const float *patch_dem;  // [tiles, 128, 128] (zero outside the valid rect)
+    const float *horizons;   // [tiles, 128, 128, 1440] degrees
+    const float *vectors;    // [T, 3] float32 Moon-ME metres
+    float *frames;           // [tiles, 16384, 12]
+    void *out;               // [tiles, time_count, 16384] (PSR: [tiles, 16384])
+    int time_start, time_count, chunk;
+};
+
+void lighting_launch(ls200_context *ctx, LightingBatch &batch, int tiles, int signal);
+void sun_fraction_launch(ls200_context *ctx, const float *horizons, const float *azimuth_deg,
+                         const float *elevation_deg, int n, float *out);
+void ensure_lighting_constants(ls200_context *ctx);
+
+#ifdef LS200_LIGHTING_KERNELS
+// Slice half-heights and their normaliser (set by ensure_lighting_constants).
+__constant__ float c_half_circle[16];
+__constant__ float c_max_photons;
+
+constexpr float kRadToDeg = 57.29577951308232f;  // float32(180/pi)
+constexpr float kTwoPi = 6.283185307179586f;      // float32(2 pi)
+
+// Azimuth (deg, [0, 360)) and elevation (deg) of a float32 Moon-ME vector in
+// a pixel's frame (lightmap_cpu.py:105-120).
+__device__ __forceinline__ void body_direction(const Frame32 &f, float vx, float vy, float vz,
+                                               float &azimuth_deg, float &elevation) {
+    const float ex = __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(vx, f.v[0]), __fmul_rn(vy, f.v[3])),
+                                         __fmul_rn(vz, f.v[6])), f.v[9]);
+    const float ey = __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(vx, f.v[1]), __fmul_rn(vy, f.v[4])),
+                                         __fmul_rn(vz, f.v[7])), f.v[10]);
+    const float ez = __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(vx, f.v[2]), __fmul_rn(vy, f.v[5])),
+                                         __fmul_rn(vz, f.v[8])), f.v[11]);
+    const float horizontal = __fsqrt_rn(__fadd_rn(__fmul_rn(ex, ex), __fmul_rn(ey, ey)));
+    elevation = __fmul_rn(atan2f(ez, horizontal), kRadToDeg);
+    float azimuth = atan2f(ex, ey);
+    if (azimuth < 0.0f) azimuth = __fadd_rn(azimuth, kTwoPi);
+    azimuth_deg = __fmul_rn(azimuth, kRadToDeg);
+}
+
+// Body-centre elevation minus the horizon interpolated at its azimuth
+// (lightmap_cpu.py:121-141).
+__device__ __forceinline__ float horizon_margin(const float *horizon, float azimuth_deg,
+                                                float elevation) {
+    const float position = __fmul_rn(azimuth_deg, 4.0f);
+    int left = static_cast<int>(position);
+    const float fraction = __fsub_rn(position, static_cast<float>(left));
+    if (left >= kAzimuths) left -= kAzimuths;
+    const int right = left + 1 >= kAzimuths ? 0 : left + 1;
+    const float hl = __ldg(horizon + left), hr = __ldg(horizon + right);
+    return __fsub_rn(elevation, __fadd_rn(hl, __fmul_rn(fraction, __fsub_rn(hr, hl))));
+}
+
+// Visible fraction of the solar disk: 16 vertical slices of a 0.27-deg disk
+// against the linearly interpolated horizon, float32 accumulation
+// (lightmap.py:32-73, lightmap_cpu.py:142-183).
+//
+// Exact shortcut: the 16 slices read bins left .. left+4 and interpolate (or,
+// for the first slices, extrapolate by less than one bin) between them, so
+// every slice's horizon lies within [min - span, max + span] of those bins.
+// When that interval is clear of the whole disk by 1e-3 deg (far above the
+// float32 rounding of degrees), every slice is fully lit (the float32 sum of
+// the 2c_k is then exactly the normaliser: fraction 1) or fully dark
+// (fraction 0), and the loop is skipped.
+__device__ __forceinline__ float sun_fraction(const float *horizon, float azimuth_deg,
+                                              float elevation) {
+    const float left_position = __fmul_rn(__fsub_rn(__fsub_rn(azimuth_deg, 0.27f), 0.125f), 4.0f);
+    int left = static_cast<int>(left_position);
+    float fraction = __fsub_rn(left_position, static_cast<float>(left));
+    if (left < 0) left += kAzimuths;
+    else if (left >= kAzimuths) left -= kAzimuths;
+    int right = left + 1 >= kAzimuths ? 0 : left + 1;
+    {
+        float lo = __ldg(horizon + left), hi = lo;
+#pragma unroll
+        for (int k = 1; k <= 4; ++k) {
+            int b = left + k;
+            if (b >= kAzimuths) b -= kAzimuths;
+            const float h = __ldg(horizon + b);
+            lo = fminf(lo, h);
+            hi = fmaxf(hi, h);
+        }
+        const float span = hi - lo;
+        const float cmax = c_half_circle[7];
+        if (hi + span <= elevation - cmax - 1e-3f) return 1.0f;
+        if (lo - span >= elevation + cmax + 1e-3f) return 0.0f;
+    }
+    float left_elevation = __ldg(horizon + left);
+    float right_elevation = __ldg(horizon + right);
+    float delta = __fsub_rn(right_elevation, left_elevation);
+    float photons = 0.0f;
+#pragma unroll
+    for (int slice = 0; slice < 16; ++slice) {
+        const float h = __fadd_rn(__fmul_rn(fraction, delta), left_elevation);
+        const float column = c_half_circle[slice];
+        const float sun_top = __fadd_rn(elevation, column);
+        if (h < sun_top) {
+            float angle = __fsub_rn(sun_top, h);
+            const float height = __fadd_rn(column, column);
+            if (angle > height) angle = height;
+            photons = __fadd_rn(photons, angle);
+        }
+        fraction = __fadd_rn(fraction, 0.135f);
+        if (fraction >= 1.0f) {
+            right = right + 1 >= kAzimuths ? 0 : right + 1;
+            left_elevation = right_elevation;
+            right_elevation = __ldg(horizon + right);
+            delta = __fsub_rn(right_elevation, left_elevation);
+            fraction = __fsub_rn(fraction, 1.0f);
+        }
+    }
+    return __fdiv_rn(photons, c_max_photons);
+}
+#endif
+
+}  // namespace ls200

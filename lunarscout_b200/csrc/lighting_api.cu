@@ -1,0 +1,231 @@
+// C-ABI entry points of the lighting products.
+#include "lighting.cuh"
+
+struct ls200_vectors {
+    ls200_context *ctx = nullptr;
+    float *data = nullptr;  // device [count, 3]
+    int count = 0;
+};
+
+namespace ls200 {
+
+struct LightingState {
+    DeviceBuffer dem, horizons, frames, out;
+    TileGeo geo{};
+    bool loaded = false;
+    std::set<ls200_vectors *> vectors;  // live vector tables of the context
+};
+
+static LightingState &state_of(ls200_context *ctx) {
+    if (!ctx->lighting) ctx->lighting = new LightingState();
+    return *ctx->lighting;
+}
+
+void release_lighting_state(ls200_context *ctx) {
+    if (!ctx->lighting) return;
+    for (ls200_vectors *v : ctx->lighting->vectors) {
+        cudaFree(v->data);
+        delete v;
+    }
+    delete ctx->lighting;
+    ctx->lighting = nullptr;
+}
+
+static void check_valid(int valid_width, int valid_height) {
+    LS_REQUIRE(valid_width >= 1 && valid_width <= kPatch && valid_height >= 1 &&
+                   valid_height <= kPatch,
+               "valid patch dimensions must be between 1 and 128");
+}
+
+static LightingBatch single_batch(LightingState &st, const ls200_vectors *v) {
+    LightingBatch B{};
+    B.tiles[0] = st.geo;
+    B.patch_dem = st.dem.as<float>();
+    B.horizons = st.horizons.as<float>();
+    B.vectors = v ? v->data : nullptr;
+    B.frames = st.frames.as<float>();
+    return B;
+}
+
+}  // namespace ls200
+
+using namespace ls200;
+
+extern "C" {
+
+ls200_status ls200_vectors_create(ls200_context *ctx, const float *vectors, int count,
+                                  ls200_vectors **out) {
+    return guard([&] {
+        LS_REQUIRE(ctx && vectors && out, "NULL argument");
+        LS_REQUIRE(count > 0, "at least one vector is required");
+        std::lock_guard<std::mutex> hold(ctx->lock);
+        activate(ctx);
+        auto v = new ls200_vectors();
+        v->ctx = ctx;
+        v->count = count;
+        cudaError_t e = cudaMalloc(&v->data, sizeof(float) * 3 * size_t(count));
+        if (e != cudaSuccess) {
+            delete v;
+            throw Error(LS200_ERR_CUDA, std::string("cudaMalloc: ") + cudaGetErrorString(e));
+        }
+        e = cudaMemcpyAsync(v->data, vectors, sizeof(float) * 3 * size_t(count),
+                            cudaMemcpyHostToDevice, ctx->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+        if (e != cudaSuccess) {
+            cudaFree(v->data);
+            delete v;
+            throw Error(LS200_ERR_CUDA, std::string("vector upload: ") + cudaGetErrorString(e));
+        }
+        state_of(ctx).vectors.insert(v);
+        *out = v;
+    });
+}
+
+ls200_status ls200_vectors_destroy(ls200_vectors *vectors) {
+    return guard([&] {
+        if (!vectors) return;
+        std::lock_guard<std::mutex> hold(vectors->ctx->lock);
+        activate(vectors->ctx);
+        cudaStreamSynchronize(vectors->ctx->stream);
+        state_of(vectors->ctx).vectors.erase(vectors);
+        cudaFree(vectors->data);
+        delete vectors;
+    });
+}
+
+ls200_status ls200_lighting_load(ls200_context *ctx, const float *patch_dem,
+                                 const double *geo_transform, const double *projection,
+                                 const float *horizons, int tile_x, int tile_y,
+                                 int valid_width, int valid_height) {
+    return guard([&] {
+        LS_REQUIRE(ctx && patch_dem && geo_transform && projection && horizons, "NULL argument");
+        check_valid(valid_width, valid_height);
+        std::lock_guard<std::mutex> hold(ctx->lock);
+        activate(ctx);
+        LightingState &st = state_of(ctx);
+        const size_t plane = size_t(kPatch) * kPatch;
+        st.dem.reserve(sizeof(float) * plane);
+        st.horizons.reserve(sizeof(float) * plane * kAzimuths);
+        st.frames.reserve(sizeof(float) * plane * 12);
+        LS_CUDA(cudaMemcpyAsync(st.dem.ptr, patch_dem, sizeof(float) * plane,
+                                cudaMemcpyHostToDevice, ctx->stream));
+        LS_CUDA(cudaMemcpyAsync(st.horizons.ptr, horizons, sizeof(float) * plane * kAzimuths,
+                                cudaMemcpyHostToDevice, ctx->stream));
+        std::memcpy(st.geo.gt, geo_transform, sizeof st.geo.gt);
+        std::memcpy(st.geo.proj, projection, sizeof st.geo.proj);
+        st.geo.tile_x = tile_x;
+        st.geo.tile_y = tile_y;
+        st.geo.valid_width = valid_width;
+        st.geo.valid_height = valid_height;
+        st.loaded = true;
+    });
+}
+
+ls200_status ls200_lighting_run(ls200_context *ctx, const ls200_vectors *vectors,
+                                int time_start, int time_count, int signal, void *out) {
+    return guard([&] {
+        LS_REQUIRE(ctx && vectors && out, "NULL argument");
+        LS_REQUIRE(signal >= kSignalFraction && signal <= kSignalMargin, "unknown signal");
+        LS_REQUIRE(time_start >= 0 && time_count > 0 && time_start + time_count <= vectors->count,
+                   "time range outside the vector table");
+        std::lock_guard<std::mutex> hold(ctx->lock);
+        activate(ctx);
+        LightingState &st = state_of(ctx);
+        LS_REQUIRE(st.loaded, "no lighting tile is loaded");
+        const size_t plane = size_t(kPatch) * kPatch;
+        const size_t item = signal == kSignalBytes ? 1 : sizeof(float);
+        const size_t bytes = item * plane * size_t(time_count);
+        st.out.reserve(bytes);
+        LightingBatch B = single_batch(st, vectors);
+        B.out = st.out.ptr;
+        B.time_start = time_start;
+        B.time_count = time_count;
+        lighting_launch(ctx, B, 1, signal);
+        LS_CUDA(cudaMemcpyAsync(out, st.out.ptr, bytes, cudaMemcpyDeviceToHost, ctx->stream));
+        LS_CUDA(cudaStreamSynchronize(ctx->stream));
+    });
+}
+
+ls200_status ls200_psr_run(ls200_context *ctx, const ls200_vectors *vectors, uint8_t *out) {
+    return guard([&] {
+        LS_REQUIRE(ctx && vectors && out, "NULL argument");
+        std::lock_guard<std::mutex> hold(ctx->lock);
+        activate(ctx);
+        LightingState &st = state_of(ctx);
+        LS_REQUIRE(st.loaded, "no lighting tile is loaded");
+        const size_t plane = size_t(kPatch) * kPatch;
+        st.out.reserve(plane);
+        LightingBatch B = single_batch(st, vectors);
+        B.out = st.out.ptr;
+        B.time_start = 0;
+        B.time_count = vectors->count;
+        lighting_launch(ctx, B, 1, kSignalPsr);
+        LS_CUDA(cudaMemcpyAsync(out, st.out.ptr, plane, cudaMemcpyDeviceToHost, ctx->stream));
+        LS_CUDA(cudaStreamSynchronize(ctx->stream));
+    });
+}
+
+ls200_status ls200_lighting_device(ls200_context *ctx, int tile_count, const float *patch_dems,
+                                   const double *geo_transforms, const double *projections,
+                                   const int32_t *windows, const float *horizons,
+                                   const ls200_vectors *vectors, int time_start,
+                                   int time_count, int signal, float *frames, void *out) {
+    return guard([&] {
+        LS_REQUIRE(ctx && patch_dems && geo_transforms && projections && windows && horizons &&
+                       vectors && frames && out,
+                   "NULL argument");
+        LS_REQUIRE(tile_count >= 1 && tile_count <= kMaxBatchTiles,
+                   "tile_count must be between 1 and 32");
+        LS_REQUIRE(signal >= kSignalFraction && signal <= kSignalPsr, "unknown signal");
+        LS_REQUIRE(time_start >= 0 && time_count > 0 && time_start + time_count <= vectors->count,
+                   "time range outside the vector table");
+        std::lock_guard<std::mutex> hold(ctx->lock);
+        activate(ctx);
+        LightingBatch B{};
+        for (int t = 0; t < tile_count; ++t) {
+            std::memcpy(B.tiles[t].gt, geo_transforms + 6 * t, sizeof B.tiles[t].gt);
+            std::memcpy(B.tiles[t].proj, projections + 6 * t, sizeof B.tiles[t].proj);
+            B.tiles[t].tile_x = windows[4 * t + 0];
+            B.tiles[t].tile_y = windows[4 * t + 1];
+            B.tiles[t].valid_width = windows[4 * t + 2];
+            B.tiles[t].valid_height = windows[4 * t + 3];
+            check_valid(B.tiles[t].valid_width, B.tiles[t].valid_height);
+        }
+        B.patch_dem = patch_dems;
+        B.horizons = horizons;
+        B.vectors = vectors->data;
+        B.frames = frames;
+        B.out = out;
+        B.time_start = signal == kSignalPsr ? 0 : time_start;
+        B.time_count = signal == kSignalPsr ? vectors->count : time_count;
+        lighting_launch(ctx, B, tile_count, signal);
+    });
+}
+
+ls200_status ls200_sun_fraction(ls200_context *ctx, const float *horizons,
+                                const float *azimuth_deg, const float *elevation_deg, int n,
+                                float *out) {
+    return guard([&] {
+        LS_REQUIRE(ctx && horizons && azimuth_deg && elevation_deg && out && n > 0,
+                   "invalid arguments");
+        std::lock_guard<std::mutex> hold(ctx->lock);
+        activate(ctx);
+        const size_t rows = sizeof(float) * size_t(n) * kAzimuths;
+        ctx->scratch.reserve(rows + 3 * sizeof(float) * size_t(n));
+        float *d_h = ctx->scratch.as<float>();
+        float *d_a = d_h + size_t(n) * kAzimuths;
+        float *d_e = d_a + n;
+        float *d_o = d_e + n;
+        LS_CUDA(cudaMemcpyAsync(d_h, horizons, rows, cudaMemcpyHostToDevice, ctx->stream));
+        LS_CUDA(cudaMemcpyAsync(d_a, azimuth_deg, sizeof(float) * n, cudaMemcpyHostToDevice,
+                                ctx->stream));
+        LS_CUDA(cudaMemcpyAsync(d_e, elevation_deg, sizeof(float) * n, cudaMemcpyHostToDevice,
+                                ctx->stream));
+        sun_fraction_launch(ctx, d_h, d_a, d_e, n, d_o);
+        LS_CUDA(cudaMemcpyAsync(out, d_o, sizeof(float) * n, cudaMemcpyDeviceToHost,
+                                ctx->stream));
+        LS_CUDA(cudaStreamSynchronize(ctx->stream));
+    });
+}
+
+}  // extern "C"

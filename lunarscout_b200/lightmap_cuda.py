@@ -1,0 +1,187 @@
+"""Drop-in ``LightmapCudaSession`` (src/lunarscout/_numba_horizon/lightmap_cuda.py:187-276).
+
+Same constructor, ``iter_patch_tiles`` / ``iter_patch_fraction_tiles`` /
+``iter_patch_margin_tiles`` signatures, lazily yielded per-time tiles and
+error behaviour.  One device launch covers a large block of time steps (all
+pixels x many times fill the GPU); host output stays bounded by that block.
+"""
+
+from __future__ import annotations
+
+import ctypes
+import hashlib
+import threading
+from collections.abc import Iterator
+
+import numpy as np
+
+from . import _native
+from ._native import CudaBackendError, call, library, register
+from .contract import AZIMUTH_COUNT, PATCH_SIZE, projection_array
+
+SIGNAL_FRACTION = 0
+SIGNAL_BYTES = 1
+SIGNAL_MARGIN = 2
+SIGNAL_PSR = 3
+#: Time steps computed per device launch by the iterators.
+DEVICE_TIME_BLOCK = 1024
+
+__all__ = ["LightmapCudaSession", "CudaBackendError"]
+
+
+def validate_vectors(vectors_m) -> np.ndarray:
+    """float64 (time, 3), finite, non-empty (psr.py:17-26)."""
+    values = np.ascontiguousarray(vectors_m, dtype=np.float64)
+    if (values.ndim != 2 or values.shape[1:] != (3,) or values.shape[0] == 0
+            or not np.all(np.isfinite(values))):
+        raise ValueError("Moon-ME vectors must be finite values shaped (time, 3)")
+    return values
+
+
+def patch_elevations(dem, tile_y, tile_x, valid_height, valid_width) -> np.ndarray:
+    patch = np.zeros((PATCH_SIZE, PATCH_SIZE), dtype=np.float32)
+    patch[:valid_height, :valid_width] = dem.elevation_m[
+        tile_y:tile_y + valid_height, tile_x:tile_x + valid_width]
+    return patch
+
+
+class DeviceVectors:
+    """A float32 vector table resident on the device."""
+
+    def __init__(self, context, vectors32: np.ndarray):
+        self._context = context
+        self.handle = ctypes.c_void_p()
+        self.count = len(vectors32)
+        call("ls200_vectors_create", context, np.ascontiguousarray(vectors32, np.float32),
+             self.count, ctypes.byref(self.handle))
+
+    def close(self, context_alive: bool = True) -> None:
+        if self.handle and context_alive:
+            library().ls200_vectors_destroy(self.handle)
+        self.handle = ctypes.c_void_p()
+
+
+class LightingContext:
+    """Owns one ls200 context for a lighting session."""
+
+    def __init__(self, device_id: int):
+        handle = ctypes.c_void_p()
+        lib = library()
+        _native.check(lib.ls200_context_create(int(device_id), ctypes.byref(handle)),
+                      "CUDA session")
+        self.handle = handle
+        self.lock = threading.Lock()
+        self.vectors: DeviceVectors | None = None
+        self.vector_key = None
+
+    def resident_vectors(self, vectors32: np.ndarray, key) -> DeviceVectors:
+        if self.vectors is None or self.vector_key != key:
+            if self.vectors is not None:
+                self.vectors.close()
+            self.vectors = DeviceVectors(self.handle, vectors32)
+            self.vector_key = key
+        return self.vectors
+
+    def close(self) -> None:
+        if self.handle:
+            if self.vectors is not None:
+                self.vectors.close()
+                self.vectors = None
+            library().ls200_context_destroy(self.handle)
+            self.handle = ctypes.c_void_p()
+
+
+class LightmapCudaSession:
+    """Sun fraction / margin tiles of one horizon patch on the B200."""
+
+    def __init__(self, *, device_id: int = 0, time_batch_size: int = 32) -> None:
+        if time_batch_size < 1:
+            raise ValueError("time_batch_size must be positive")
+        self.time_batch_size = int(time_batch_size)
+        self._context = LightingContext(device_id)
+        self._lock = threading.Lock()
+
+    def close(self) -> None:
+        self._context.close()
+
+    def __del__(self):  # pragma: no cover
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def _iter_patch_batches(self, dem, horizons_deg, body_vectors_m, *, tile_y: int,
+                            tile_x: int, valid_height: int, valid_width: int, signal: str):
+        vectors64 = validate_vectors(body_vectors_m)
+        vectors = np.ascontiguousarray(vectors64, dtype=np.float32)
+        horizons = np.ascontiguousarray(horizons_deg, dtype=np.float32)
+        if horizons.shape != (PATCH_SIZE, PATCH_SIZE, AZIMUTH_COUNT):
+            raise ValueError("horizons must have shape (128, 128, 1440)")
+        if not 1 <= valid_width <= PATCH_SIZE or not 1 <= valid_height <= PATCH_SIZE:
+            raise ValueError("valid patch dimensions must be between 1 and 128")
+        patch = patch_elevations(dem, tile_y, tile_x, valid_height, valid_width)
+        geo = np.ascontiguousarray(dem.geo_transform, dtype=np.float64)
+        projection = projection_array(dem.projection)
+        key = hashlib.sha256(vectors.tobytes()).digest()
+        code = {"fraction": SIGNAL_FRACTION, "margin": SIGNAL_MARGIN,
+                "encoded": SIGNAL_BYTES}[signal]
+        dtype = np.uint8 if code == SIGNAL_BYTES else np.float32
+        total = len(vectors)
+        block = max(self.time_batch_size, DEVICE_TIME_BLOCK)
+        # Like the reference session, the lock is held for the whole patch
+        # (across yields): the device tile buffers belong to one patch.
+        with self._lock, self._context.lock:
+            device_vectors = self._context.resident_vectors(vectors, key)
+            call("ls200_lighting_load", self._context.handle, patch, geo, projection,
+                 horizons.reshape(-1), int(tile_x), int(tile_y), int(valid_width),
+                 int(valid_height))
+            for block_start in range(0, total, block):
+                count = min(block, total - block_start)
+                out = np.empty((count, PATCH_SIZE, PATCH_SIZE), dtype=dtype)
+                call("ls200_lighting_run", self._context.handle, device_vectors.handle,
+                     block_start, count, code, out.ctypes.data)
+                for start in range(0, count, self.time_batch_size):
+                    stop = min(start + self.time_batch_size, count)
+                    yield out[start:stop, :valid_height, :valid_width]
+
+    def iter_patch_fraction_tiles(self, dem, horizons_deg, sun_vectors_m, *, tile_y: int,
+                                  tile_x: int, valid_height: int = PATCH_SIZE,
+                                  valid_width: int = PATCH_SIZE) -> Iterator[np.ndarray]:
+        """float32 visible solar-disk fraction per time step."""
+        for batch in self._iter_patch_batches(
+                dem, horizons_deg, sun_vectors_m, tile_y=tile_y, tile_x=tile_x,
+                valid_height=valid_height, valid_width=valid_width, signal="fraction"):
+            for tile in batch:
+                yield np.ascontiguousarray(tile)
+
+    def iter_patch_margin_tiles(self, dem, horizons_deg, body_vectors_m, *, tile_y: int,
+                                tile_x: int, valid_height: int = PATCH_SIZE,
+                                valid_width: int = PATCH_SIZE) -> Iterator[np.ndarray]:
+        """Body-centre elevation relative to the interpolated local horizon."""
+        for batch in self._iter_patch_batches(
+                dem, horizons_deg, body_vectors_m, tile_y=tile_y, tile_x=tile_x,
+                valid_height=valid_height, valid_width=valid_width, signal="margin"):
+            for tile in batch:
+                yield np.ascontiguousarray(tile)
+
+    def iter_patch_tiles(self, dem, horizons_deg, sun_vectors_m, *, tile_y: int, tile_x: int,
+                         valid_height: int = PATCH_SIZE,
+                         valid_width: int = PATCH_SIZE) -> Iterator[np.ndarray]:
+        """uint8 lightmap bytes, int(float32(255) * fraction)."""
+        for batch in self._iter_patch_batches(
+                dem, horizons_deg, sun_vectors_m, tile_y=tile_y, tile_x=tile_x,
+                valid_height=valid_height, valid_width=valid_width, signal="encoded"):
+            for tile in batch:
+                yield np.ascontiguousarray(tile)
+
+    def sun_fraction(self, horizons: np.ndarray, azimuth_deg, elevation_deg) -> np.ndarray:
+        """Diagnostic: fraction of the disk at (azimuth, elevation) above each
+        horizon row (lightmap.py:32-73)."""
+        horizons = np.ascontiguousarray(horizons, dtype=np.float32).reshape(-1, AZIMUTH_COUNT)
+        az = np.ascontiguousarray(np.broadcast_to(azimuth_deg, (len(horizons),)), np.float32)
+        el = np.ascontiguousarray(np.broadcast_to(elevation_deg, (len(horizons),)), np.float32)
+        out = np.empty(len(horizons), dtype=np.float32)
+        with self._context.lock:
+            call("ls200_sun_fraction", self._context.handle, horizons.reshape(-1), az, el,
+                 len(horizons), out)
+        return out

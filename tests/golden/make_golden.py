@@ -259,6 +259,122 @@ def segments_halo() -> None:
     np.savez_compressed(OUT / "segments_halo.npz", **arrays)
 
 
+def lighting_csharp() -> None:
+    """C# BuilderSunFraction samples and ILGPU PSR tiles."""
+    import base64
+
+    lightmap = json.loads((DATA / "phase6b_lightmap_csharp.json").read_text())
+    arrays = {}
+    for index, case in enumerate(lightmap["cases"]):
+        arrays[f"lm{index}_horizon"] = np.frombuffer(
+            base64.b64decode(case["horizons_float32_base64"]), dtype="<f4").astype(np.float32)
+        arrays[f"lm{index}_samples"] = np.array(
+            [[s["azimuth_deg"], s["elevation_deg"], s["encoded_byte"], s["fraction_float32_bits"]]
+             for s in case["samples"]], dtype=np.float64)
+    psr = json.loads((DATA / "phase6b_psr_csharp.json").read_text())
+    p = psr["projection"]
+    arrays["psr_geo_transform"] = np.asarray(psr["geotransform"], dtype=np.float64)
+    arrays["psr_projection"] = np.array(
+        (p["radius_m"], p["latitude_origin_rad"], p["longitude_origin_rad"], p["scale"],
+         p["false_easting_m"], p["false_northing_m"]), dtype=np.float64)
+    names = []
+    for index, case in enumerate(psr["cases"]):
+        names.append(case["name"])
+        arrays[f"psr{index}_vectors"] = np.asarray(case["sun_vectors_m"], np.float64).reshape(-1, 3)
+        arrays[f"psr{index}_expected"] = np.frombuffer(
+            base64.b64decode(case["output_base64"]), dtype=np.uint8).reshape(128, 128)
+    arrays["psr_names"] = np.array(names)
+    np.savez_compressed(OUT / "lighting_csharp.npz", **arrays)
+
+
+def synthetic_horizons(height=128, width=128):
+    """Deterministic horizon tile (degrees): smooth ridges in azimuth whose
+    phase and level vary per pixel (the level rises across the tile, so that
+    some pixels are permanently shadowed)."""
+    az = np.radians(np.arange(1440, dtype=np.float64) * 0.25)
+    y, x = np.mgrid[0:height, 0:width]
+    phase = (0.05 * x + 0.03 * y)[..., None]
+    level = (1.0 + 0.25 * (x - y))[..., None]
+    h = level + 2.5 * np.sin(3.0 * az + phase) + 1.0 * np.sin(11.0 * az + 2.0 * phase)
+    return np.ascontiguousarray(h, dtype=np.float32)
+
+
+def lighting_reference() -> None:
+    """Reference CPU backend outputs on the synthetic 512x512 site DEM."""
+    sys.path.insert(0, str(OUT.parents[1]))
+    from lunarscout._numba_horizon.lightmap_cpu import LightmapCpuSession
+    from lunarscout._numba_horizon.mission_duration import (
+        reduce_longest_candidate_duration_stream, weekly_candidate_intervals)
+    from lunarscout._numba_horizon.psr import (
+        compute_psr_patch_reference, reduce_sun_vectors_for_psr)
+    from lunarscout_b200 import synthetic
+
+    from lunarscout._numba_horizon.geometry import DemGrid, ProjectionParameters
+
+    ours = synthetic.config1_dem()
+    dem = DemGrid(ours.elevation_m, ours.geo_transform,
+                  ProjectionParameters.from_array(ours.projection.as_array()))
+    tile = dict(tile_y=448, tile_x=448, valid_height=40, valid_width=48)
+    horizons = np.zeros((128, 128, 1440), dtype=np.float32)
+    horizons[:] = synthetic_horizons()
+    hours = synthetic.hours_between("2029-01-01T00", "2029-02-01T00", 6.0)
+    sun = synthetic.sun_vectors(hours)
+    earth = synthetic.earth_vectors(hours)
+    session = LightmapCpuSession(time_batch_size=32)
+    fractions = np.stack(list(session.iter_patch_fraction_tiles(dem, horizons, sun, **tile)))
+    margins = np.stack(list(session.iter_patch_margin_tiles(dem, horizons, earth, **tile)))
+    reduced, indices = reduce_sun_vectors_for_psr(dem, sun)
+    psr = compute_psr_patch_reference(dem, horizons, reduced, **tile)
+    psr_all = compute_psr_patch_reference(dem, horizons, sun, **tile)
+    times = [f"2029-01-01T00:00:00+00:00"] * 0
+    import datetime as dt
+
+    start = dt.datetime(2029, 1, 1, tzinfo=dt.timezone.utc)
+    times = [start + dt.timedelta(hours=float(h)) for h in hours]
+    stop = start + dt.timedelta(days=31, hours=6)
+    intervals = weekly_candidate_intervals(start, stop)
+    durations = reduce_longest_candidate_duration_stream(
+        (f >= np.float32(0.5) for f in fractions), times_utc=times, evaluation_start_utc=start,
+        evaluation_stop_utc=stop, start_intervals=intervals, output_unit="hours")
+    both = reduce_longest_candidate_duration_stream(
+        ((f >= np.float32(0.5)) & (m >= np.float32(0.0)) for f, m in zip(fractions, margins)),
+        times_utc=times, evaluation_start_utc=start, evaluation_stop_utc=stop,
+        start_intervals=intervals, output_unit="days")
+    np.savez_compressed(
+        OUT / "lighting_reference.npz",
+        tile=np.array([tile["tile_y"], tile["tile_x"], tile["valid_height"], tile["valid_width"]]),
+        hours=hours, fractions=fractions.astype(np.float32), margins=margins.astype(np.float32),
+        psr_reduced_indices=indices, psr_reduced=psr, psr_all=psr_all,
+        durations_hours=np.stack(durations), durations_days_sun_earth=np.stack(both),
+        interval_bounds_hours=np.array(
+            [[(i.start_utc - start).total_seconds() / 3600.0,
+              (i.stop_utc - start).total_seconds() / 3600.0] for i in intervals]),
+        evaluation_stop_hours=np.float64((stop - start).total_seconds() / 3600.0),
+    )
+
+
+def codec_reference() -> None:
+    """The reference .cbin encoder on a deterministic degree tile."""
+    import hashlib
+
+    from lunarscout._numba_horizon.file_format import _decode_compressed_payload, _encode_horizons
+
+    degrees = synthetic_horizons().reshape(-1, 1440) * np.float32(6.0)
+    degrees[5, :7] = -np.inf          # sentinel pixels encode as -50
+    degrees[9, 100:110] = 75.0        # clamps at +50
+    encoded, lengths = _encode_horizons(np.ascontiguousarray(degrees, dtype=np.float32))
+    payload = b"".join(int(n).to_bytes(2, "little") + encoded[i, :n].tobytes()
+                       for i, n in enumerate(lengths))
+    decoded = _decode_compressed_payload(np.frombuffer(payload, dtype=np.uint8))
+    np.savez_compressed(
+        OUT / "codec_reference.npz",
+        payload_sha256=np.array(hashlib.sha256(payload).hexdigest()),
+        payload_size=np.int64(len(payload)), lengths=lengths.astype(np.uint16),
+        head=np.frombuffer(payload[:4096], dtype=np.uint8),
+        decoded_rows=decoded[[0, 5, 9, 777, 16383]],
+    )
+
+
 def main() -> None:
     parser = argparse.ArgumentParser()
     parser.add_argument("--simulate", action="store_true")
@@ -269,6 +385,9 @@ def main() -> None:
         "horizon": lambda: horizon_production(args.simulate),
         "pyramids": pyramids_fixture,
         "segments": segments_halo,
+        "lighting_csharp": lighting_csharp,
+        "lighting_reference": lighting_reference,
+        "codec": codec_reference,
     }
     for name, job in jobs.items():
         if args.only and name not in args.only.split(","):

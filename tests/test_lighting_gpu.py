@@ -1,0 +1,146 @@
+"""Lightmap (fraction, bytes, margin) and PSR on the B200 vs the oracle.
+
+Tolerances are the north-star bars: sun fraction within 1e-4 absolute of the
+reference CPU backend; PSR bit-exact except a counted band of pixels whose
+peak (sun centre - horizon) lies within 1e-4 deg of the -0.2725 deg limb
+threshold.  Differences come only from CUDA's atan2f vs glibc's.
+"""
+
+from __future__ import annotations
+
+import numpy as np
+import pytest
+
+from oracle import products
+from conftest import load_golden
+from test_oracle_lighting_pins import _csharp_psr_inputs, synthetic_horizons
+
+pytestmark = pytest.mark.gpu
+
+FRACTION_TOL = 1e-4
+MARGIN_TOL = 1e-4
+BAND_DEG = 1e-4
+
+
+@pytest.fixture(scope="module")
+def lighting_session():
+    from lunarscout_b200.lightmap_cuda import LightmapCudaSession
+
+    session = LightmapCudaSession(time_batch_size=32)
+    yield session
+    session.close()
+
+
+@pytest.fixture(scope="module")
+def psr_session():
+    from lunarscout_b200.psr_cuda import PsrCudaSession
+
+    session = PsrCudaSession()
+    yield session
+    session.close()
+
+
+@pytest.fixture(scope="module")
+def site():
+    from lunarscout_b200 import synthetic
+
+    hours = synthetic.hours_between("2029-01-01T00", "2029-02-01T00", 6.0)
+    return dict(dem=synthetic.config1_dem(), horizons=synthetic_horizons(),
+                sun=synthetic.sun_vectors(hours), earth=synthetic.earth_vectors(hours),
+                tile=dict(tile_y=448, tile_x=448, valid_height=40, valid_width=48))
+
+
+def test_sun_fraction_kernel_is_bit_identical_on_csharp_samples(lighting_session):
+    arrays = load_golden("lighting_csharp.npz")
+    for index in range(3):
+        horizon = arrays[f"lm{index}_horizon"]
+        samples = arrays[f"lm{index}_samples"]
+        rows = np.repeat(horizon[None, :], len(samples), axis=0)
+        gpu = lighting_session.sun_fraction(rows, samples[:, 0], samples[:, 1])
+        cpu = products.sun_fraction(rows, samples[:, 0], samples[:, 1])
+        np.testing.assert_array_equal(gpu, cpu)
+        np.testing.assert_array_equal((np.float32(255) * gpu).astype(np.uint8),
+                                      samples[:, 2].astype(np.uint8))
+
+
+def test_fraction_tiles_match_reference_cpu_backend(lighting_session, site):
+    tiles = list(lighting_session.iter_patch_fraction_tiles(
+        site["dem"], site["horizons"], site["sun"], **site["tile"]))
+    assert len(tiles) == len(site["sun"])
+    assert tiles[0].shape == (40, 48) and tiles[0].dtype == np.float32
+    gpu = np.stack(tiles)
+    cpu = products.lighting_tiles(site["dem"], site["horizons"], site["sun"], **site["tile"])
+    error = np.abs(gpu - cpu)
+    assert error.max() <= FRACTION_TOL, error.max()
+    assert np.mean(gpu == cpu) > 0.9
+
+
+def test_byte_tiles_differ_by_at_most_one_count(lighting_session, site):
+    gpu = np.stack(list(lighting_session.iter_patch_tiles(
+        site["dem"], site["horizons"], site["sun"], **site["tile"])))
+    assert gpu.dtype == np.uint8
+    cpu = products.encode_fraction_bytes(
+        products.lighting_tiles(site["dem"], site["horizons"], site["sun"], **site["tile"]))
+    diff = np.abs(gpu.astype(np.int16) - cpu.astype(np.int16))
+    assert diff.max() <= 1
+    assert np.count_nonzero(diff) <= 0.001 * diff.size
+
+
+def test_margin_tiles_match_reference_cpu_backend(lighting_session, site):
+    gpu = np.stack(list(lighting_session.iter_patch_margin_tiles(
+        site["dem"], site["horizons"], site["earth"], **site["tile"])))
+    cpu = products.lighting_tiles(site["dem"], site["horizons"], site["earth"], margin=True,
+                                  **site["tile"])
+    assert np.abs(gpu - cpu).max() <= MARGIN_TOL
+
+
+def test_full_tile_and_time_blocks_longer_than_one_launch(lighting_session, site):
+    from lunarscout_b200 import synthetic
+
+    hours = synthetic.hours_between("2029-01-01T00", "2029-03-15T00", 1.0)[:1500]
+    vectors = synthetic.sun_vectors(hours)
+    tile = dict(tile_y=128, tile_x=256)
+    gpu = np.stack(list(lighting_session.iter_patch_fraction_tiles(
+        site["dem"], site["horizons"], vectors, **tile)))
+    assert gpu.shape == (1500, 128, 128)
+    picks = np.array([0, 1, 31, 32, 1023, 1024, 1499])
+    cpu = products.lighting_tiles(site["dem"], site["horizons"], vectors[picks], **tile)
+    assert np.abs(gpu[picks] - cpu).max() <= FRACTION_TOL
+
+
+def test_psr_matches_oracle_outside_the_threshold_band(psr_session, site):
+    _, indices = products.reduce_sun_vectors(site["dem"], site["sun"])
+    reduced = site["sun"][indices]
+    gpu = psr_session.compute_patch(site["dem"], site["horizons"], reduced, **site["tile"])
+    cpu = products.psr_tile(site["dem"], site["horizons"], reduced, **site["tile"])
+    peak = products.psr_peak_margin(site["dem"], site["horizons"], reduced, **site["tile"])
+    band = np.abs(peak - products.PSR_LIMB_THRESHOLD) < BAND_DEG
+    mismatched = gpu != cpu
+    assert not np.any(mismatched & ~band), np.argwhere(mismatched & ~band)[:5]
+    assert 0 < np.count_nonzero(gpu == 255) < gpu.size
+
+
+def test_psr_matches_csharp_ilgpu_tiles(psr_session):
+    from lunarscout_b200.contract import DemGrid
+
+    arrays = load_golden("lighting_csharp.npz")
+    for index, name in enumerate(str(n) for n in arrays["psr_names"]):
+        dem, horizons = _csharp_psr_inputs(arrays, name)
+        vectors = arrays[f"psr{index}_vectors"]
+        gpu = psr_session.compute_patch(dem, horizons, vectors, tile_y=0, tile_x=0)
+        expected = arrays[f"psr{index}_expected"]
+        peak = products.psr_peak_margin(dem, horizons, vectors, tile_y=0, tile_x=0)
+        band = np.abs(peak - products.PSR_LIMB_THRESHOLD) < BAND_DEG
+        assert not np.any((gpu != expected) & ~band), name
+
+
+def test_psr_pinned_buffer_and_validation(psr_session, site):
+    buffer = psr_session.allocate_pinned_horizon_buffer()
+    assert buffer.shape == (128, 128, 1440) and buffer.dtype == np.float32
+    buffer[...] = site["horizons"]
+    out = psr_session.compute_patch(site["dem"], buffer, site["sun"][:10], tile_y=0, tile_x=0)
+    assert out.shape == (128, 128)
+    with pytest.raises(ValueError):
+        psr_session.compute_patch(site["dem"], buffer, site["sun"][:10], tile_y=500, tile_x=0)
+    with pytest.raises(ValueError):
+        psr_session.compute_patch(site["dem"], buffer[:64], site["sun"][:10], tile_y=0, tile_x=0)

@@ -379,6 +379,8 @@ def run_ours(args):
                 "gathered_bytes_per_launch": gathered,
                 "launch_ms": march_seconds * 1000.0,
                 "node_visits_per_ray": visits / (args.steps * RAYS_PER_TILE),
+                "ray_steps_per_ray": ray_steps / (args.steps * RAYS_PER_TILE),
+                "level0_samples_per_ray": samples / (args.steps * RAYS_PER_TILE),
             },
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": "rays/s", "h2d_bytes_per_step": h2d,

@@ -91,7 +91,7 @@ ls200_status ls200_context_destroy(ls200_context *ctx) {
         // DEMs still alive belong to this context: release them with it.
         for (ls200_dem *dem : ctx->dems) {
             if (dem->level0) cudaFree(dem->level0);
-            if (dem->mips) cudaFree(dem->mips);
+            if (dem->cells) cudaFree(dem->cells);
             delete dem;
         }
         ctx->dems.clear();
@@ -177,23 +177,27 @@ ls200_status ls200_dem_create(ls200_context *ctx, const float *level0, int width
             std::memcpy(dem->geo_transform, geo_transform, sizeof dem->geo_transform);
             std::memcpy(dem->projection, projection, sizeof dem->projection);
             std::memcpy(dem->map_parameters, map_parameters, sizeof dem->map_parameters);
-            const size_t bytes0 = sizeof(float) * size_t(width) * height;
-            LS_CUDA(cudaMalloc(&dem->level0, bytes0));
-            LS_CUDA(cudaMalloc(&dem->mips, sizeof(float) * size_t(dem->mip_count > 0
-                                                                      ? dem->mip_count : 1)));
-            LS_CUDA(cudaMemcpyAsync(dem->level0, level0, bytes0, cudaMemcpyHostToDevice,
-                                    ctx->stream));
+            const size_t cells0 = size_t(width) * height;
+            LS_REQUIRE(cells0 + size_t(dem->mip_count) < (size_t(1) << 31),
+                       "DEM pyramid exceeds the int32 cell index range");
+            LS_CUDA(cudaMalloc(&dem->level0, sizeof(float) * cells0));
+            // One allocation: sanitized level 0 followed by the packed mips.
+            LS_CUDA(cudaMalloc(&dem->cells, sizeof(float) * (cells0 + size_t(dem->mip_count))));
+            dem->mips = dem->cells + cells0;
+            LS_CUDA(cudaMemcpyAsync(dem->level0, level0, sizeof(float) * cells0,
+                                    cudaMemcpyHostToDevice, ctx->stream));
             if (mips) {
                 LS_CUDA(cudaMemcpyAsync(dem->mips, mips, sizeof(float) * dem->mip_count,
                                         cudaMemcpyHostToDevice, ctx->stream));
             } else {
                 build_pyramid_device(ctx, dem);
             }
+            sanitize_level0(ctx, dem);
             LS_CUDA(cudaStreamSynchronize(ctx->stream));
             ctx->dems.insert(dem);
         } catch (...) {
             if (dem->level0) cudaFree(dem->level0);
-            if (dem->mips) cudaFree(dem->mips);
+            if (dem->cells) cudaFree(dem->cells);
             delete dem;
             throw;
         }
@@ -209,7 +213,7 @@ ls200_status ls200_dem_destroy(ls200_dem *dem) {
         cudaStreamSynchronize(dem->ctx->stream);
         dem->ctx->dems.erase(dem);
         if (dem->level0) cudaFree(dem->level0);
-        if (dem->mips) cudaFree(dem->mips);
+        if (dem->cells) cudaFree(dem->cells);
         delete dem;
     });
 }

@@ -95,8 +95,11 @@ struct ls200_dem {
     int level_count = 0;
     int64_t mip_count = 0;
     ls200::PyramidLevel levels[ls200::kMaxLevels];
-    float *level0 = nullptr;  // device [height, width]
-    float *mips = nullptr;    // device [mip_count]
+    float *level0 = nullptr;  // device [height, width], as given
+    // device [height*width + mip_count]: level 0 with every invalid value
+    // (NaN, +-inf, <= -20000) replaced by -32000, then the packed mips.
+    float *cells = nullptr;
+    float *mips = nullptr;    // = cells + height*width
     double geo_transform[6];
     double projection[6];
     float map_parameters[11];
@@ -133,6 +136,8 @@ int pyramid_layout(int width, int height, PyramidLevel *levels, int capacity,
 
 // Build all mip levels of `dem` on ctx->stream from dem->level0.
 void build_pyramid_device(ls200_context *ctx, ls200_dem *dem);
+// Write the sanitized level 0 at the start of dem->cells.
+void sanitize_level0(ls200_context *ctx, ls200_dem *dem);
 
 // Segment generation into device memory.
 void segments_device(ls200_context *ctx, ls200_dem *const *dems, int dem_count,

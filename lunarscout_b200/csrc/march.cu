@@ -11,10 +11,22 @@
 // reference's GPU compiler fuses are written as explicit __fmaf_rn:
 //   * every "x + a*b" / "x - a*b" whose product feeds the add is fused;
 //   * for "a*b + c*d" the first product is fused.
-// Division and square root are the IEEE round-to-nearest operations.  With
-// the same segment inputs the results are bit-identical to the CPU oracle's
-// FP32 restatement, which reproduces the reference's golden traversal
-// captures.
+// Division, reciprocal and square root are IEEE round-to-nearest.  With the
+// same segment inputs the results are bit-identical to the CPU oracle's FP32
+// restatement, which reproduces the reference's golden traversal captures.
+//
+// The kernel is bound by instruction issue (its gathers hit L1/L2), so the
+// work per node visit is kept small without changing any rounded value or
+// decision:
+//   * cells come from a sanitized copy of level 0 (invalid -> -32000) packed
+//     with the mips, so validity is one comparison and the four-cell bound
+//     is a plain maximum;
+//   * per-level constants (cell side, block metres, step and fallback
+//     advances, offsets) live in a shared table computed once per block;
+//   * the tangent and its reciprocals depend only on the ray position and are
+//     computed once per position, not per level;
+//   * the cull test decides with a cheap bound outside a guard band and with
+//     the reference arithmetic inside it (bound_culled).
 //
 // Layout.  Working slopes are azimuth-major [A, P] so that a warp (32
 // adjacent pixels of one tile row, one azimuth) reads and writes 128
@@ -28,14 +40,13 @@ namespace ls200 {
 struct MarchParams {
     const float *segments;  // [A, C, D, 18]
     int azimuth_count, center_count, dem_count;
-    const float *primary_level0;
+    const float *primary_cells;
     int primary_width, primary_height;
     float primary_m6, primary_m9;
-    const float *level0;
+    const float *cells;  // sanitized level 0 + mips of the active DEM
     int width, height;
-    const float *mips;
     int level_count;
-    int4 levels[kMaxLevels];  // (offset, width, height, -)
+    int4 levels[kMaxLevels];  // (cell offset, width, height, -)
     float m6, m7, m9, m10, radius;
     int tile_column, tile_row, tile_width, tile_height, subpatch, pass_index;
     float observer_elevation;
@@ -44,9 +55,15 @@ struct MarchParams {
     unsigned long long *counters;
 };
 
-__device__ __forceinline__ bool valid_elev(float v) {
-    return !isnan(v) && !isinf(v) && v > -20000.0f;
-}
+// Per-level constants shared by a block (every thread of a launch marches
+// the same DEM at the same resolution).
+struct LevelTable {
+    float side[kMaxLevels];      // float(4^l) * resolution: the level choice
+    float block_m[kMaxLevels];   // the same product (metres per cell)
+    float fallback[kMaxLevels];  // ((block_m * 0.5) * 0.001)
+    float out_step[kMaxLevels];  // max(0.001, block_m * 0.001)
+    int4 cells[kMaxLevels];      // (offset, width, height, -)
+};
 
 __device__ __forceinline__ float quartic(float x0, float a1, float a2, float a3, float a4,
                                          float d) {
@@ -68,8 +85,9 @@ __device__ __forceinline__ float quartic_tangent(float a1, float a2, float a3, f
     return __fmaf_rn(__fmul_rn(4.0f, a4), d3, r);
 }
 
-// Clamped bilinear sample; -32000 when any of the four corners is invalid.
-__device__ __forceinline__ float bilinear(const float *__restrict__ elevation, int width,
+// Clamped bilinear sample of sanitized level-0 cells; -32000 when any corner
+// is invalid (cuda_backend.py:107-132).
+__device__ __forceinline__ float bilinear(const float *__restrict__ cells, int width,
                                           int height, float column, float row) {
     const float cmax = __fsub_rn(static_cast<float>(width), 1.0001f);
     const float rmax = __fsub_rn(static_cast<float>(height), 1.0001f);
@@ -81,11 +99,11 @@ __device__ __forceinline__ float bilinear(const float *__restrict__ elevation, i
     const int y0 = static_cast<int>(floorf(row));
     const int x1 = min(x0 + 1, width - 1);
     const int y1 = min(y0 + 1, height - 1);
-    const float *r0 = elevation + static_cast<size_t>(y0) * width;
-    const float *r1 = elevation + static_cast<size_t>(y1) * width;
+    const float *r0 = cells + static_cast<size_t>(y0) * width;
+    const float *r1 = cells + static_cast<size_t>(y1) * width;
     const float q00 = __ldg(r0 + x0), q10 = __ldg(r0 + x1);
     const float q01 = __ldg(r1 + x0), q11 = __ldg(r1 + x1);
-    if (!(valid_elev(q00) && valid_elev(q10) && valid_elev(q01) && valid_elev(q11)))
+    if (!(q00 > -20000.0f && q10 > -20000.0f && q01 > -20000.0f && q11 > -20000.0f))
         return -32000.0f;
     const float tx = __fsub_rn(column, static_cast<float>(x0));
     const float ty = __fsub_rn(row, static_cast<float>(y0));
@@ -180,7 +198,23 @@ __device__ __forceinline__ float hypot_fused(float a, float b) {
 }
 
 template <bool kCount>
-__global__ void __launch_bounds__(128) march_pass_kernel(const __grid_constant__ MarchParams P) {
+__global__ void __launch_bounds__(128, 8) march_pass_kernel(const __grid_constant__ MarchParams P) {
+    __shared__ LevelTable table;
+    const float column_res = hypot_fused(P.m6, P.m9);
+    const float row_res = hypot_fused(P.m7, P.m10);
+    const float resolution = __fmul_rn(__fadd_rn(column_res, row_res), 0.5f);
+    if (threadIdx.x < P.level_count) {
+        const int l = threadIdx.x;
+        const float block_m = __fmul_rn(static_cast<float>(1 << (2 * l)), resolution);
+        const float step_km = __fmul_rn(block_m, 0.001f);
+        table.side[l] = block_m;
+        table.block_m[l] = block_m;
+        table.fallback[l] = __fmul_rn(__fmul_rn(block_m, 0.5f), 0.001f);
+        table.out_step[l] = 0.001f > step_km ? 0.001f : step_km;
+        table.cells[l] = P.levels[l];
+    }
+    __syncthreads();
+
     const int pixel_count = P.tile_width * P.tile_height;
     const long long linear = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (linear >= static_cast<long long>(pixel_count) * P.azimuth_count) return;
@@ -196,8 +230,6 @@ __global__ void __launch_bounds__(128) march_pass_kernel(const __grid_constant__
     }
 
     // ---- subpatch interpolation (cuda_backend.py:1032-1119) ----
-    const float column_res = hypot_fused(P.m6, P.m9);
-    const float row_res = hypot_fused(P.m7, P.m10);
     const int count = P.tile_width / P.subpatch + 2;
     const float gx = __fadd_rn(__fdiv_rn(static_cast<float>(column - P.subpatch / 2),
                                          static_cast<float>(P.subpatch)), 1.0f);
@@ -260,14 +292,14 @@ __global__ void __launch_bounds__(128) march_pass_kernel(const __grid_constant__
     const float c1 = seg[13], c2 = seg[14], c3 = seg[15];
 
     const float observer_z = __fadd_rn(
-        bilinear(P.primary_level0, P.primary_width, P.primary_height,
+        bilinear(P.primary_cells, P.primary_width, P.primary_height,
                  static_cast<float>(P.tile_column + column),
                  static_cast<float>(P.tile_row + row)),
         P.observer_elevation);
-    const float resolution = __fmul_rn(__fadd_rn(column_res, row_res), 0.5f);
     const float radius = P.radius;
     const float observer_radius = __fadd_rn(radius, observer_z);
     const float inverse_denominator = __frcp_rn(__fmul_rn(2.0f, observer_radius));
+    const float *__restrict__ cells = P.cells;
 
     // ---- hierarchy_maximum (cuda_backend.py:656-874) ----
     float current = -1e30f;
@@ -280,20 +312,21 @@ __global__ void __launch_bounds__(128) march_pass_kernel(const __grid_constant__
     const float primary_far_step = __fmul_rn(__fmul_rn(0.8f, resolution), 0.001f);
     const float last_x = static_cast<float>(P.width - 1);
     const float last_y = static_cast<float>(P.height - 1);
+    const int top_level = P.level_count - 1;
     unsigned visits = 0, samples = 0, steps = 0;
-    bool ray_out = false;
     while (s <= s_end) {
         if (kCount) ++steps;
         const float delta = __fsub_rn(s, s_start);
         const float px = quartic(start_x, a1, a2, a3, a4, delta);
         const float py = quartic(start_y, b1, b2, b3, b4, delta);
-        if (isnan(px) || isnan(py) || px < 0.0f || py < 0.0f || px >= last_x || py >= last_y)
-            break;
+        // NaN fails every comparison, as the reference's isnan tests do.
+        if (!(px >= 0.0f && py >= 0.0f && px < last_x && py < last_y)) break;
         const float planar_x = __fmul_rn(__fsub_rn(px, start_x), resolution);
         const float planar_y = __fmul_rn(__fsub_rn(py, start_y), resolution);
         const float planar_m = hypot_fused(planar_x, planar_y);
+        const bool near = s < 0.5f;
         float true_m;
-        if (s < 0.5f) {
+        if (near) {
             true_m = __fmul_rn(s, 1000.0f);
         } else {
             const float pm2 = __fmul_rn(planar_m, planar_m);
@@ -303,57 +336,36 @@ __global__ void __launch_bounds__(128) march_pass_kernel(const __grid_constant__
             true_m = __fmaf_rn(s_start_chord, 1000.0f, chord);
         }
         const float footprint = __fmul_rn(true_m, 0.004363323129985824f);
-        int level = P.level_count - 1;
-        while (level > 0) {
-            const float side = __fmul_rn(static_cast<float>(1 << (level * 2)), resolution);
-            if (side <= footprint) break;
-            --level;
-        }
-        // The tangent and its reciprocals depend only on delta: computed once
-        // per ray position, they are the values every level visit would
-        // recompute.
+        int level = top_level;
+        while (level > 0 && !(table.side[level] <= footprint)) --level;
+        // The tangent and its reciprocals depend only on delta.
         const float dx = quartic_tangent(a1, a2, a3, a4, delta);
         const float dy = quartic_tangent(b1, b2, b3, b4, delta);
-        const float inv_x = fabsf(dx) > 1e-8f ? __fdiv_rn(1.0f, dx) : 1e30f;
-        const float inv_y = fabsf(dy) > 1e-8f ? __fdiv_rn(1.0f, dy) : 1e30f;
+        const float inv_x = fabsf(dx) > 1e-8f ? __frcp_rn(dx) : 1e30f;
+        const float inv_y = fabsf(dy) > 1e-8f ? __frcp_rn(dy) : 1e30f;
         const int ipx = static_cast<int>(px), ipy = static_cast<int>(py);
-        while (level >= 0) {
-            const int4 L = P.levels[level];
+        bool ray_out = false;
+        for (;;) {
+            const int4 L = table.cells[level];
             const int shift = level * 2;
-            const int scale = 1 << shift;
             const int cx = ipx >> shift, cy = ipy >> shift;
-            const float scale_f = static_cast<float>(scale);
-            const float block_m = __fmul_rn(scale_f, resolution);
             if (kCount) ++visits;
-            if (!(0 <= cx && cx < L.y && 0 <= cy && cy < L.z)) {
-                const float step_km = __fmul_rn(block_m, 0.001f);
-                s = __fadd_rn(s, 0.001f > step_km ? 0.001f : step_km);
+            if (cx >= L.y || cy >= L.z) {  // cx, cy >= 0 since px, py >= 0
+                s = __fadd_rn(s, table.out_step[level]);
                 ray_out = true;
                 break;
             }
             // Four-cell bound of every bilinear sample cornered in this cell.
-            float maximum_height = -32000.0f;
-            {
-                const bool has_right = cx + 1 < L.y, has_down = cy + 1 < L.z;
-                const float *cell = level == 0 ? P.level0 + static_cast<size_t>(cy) * L.y + cx
-                                               : P.mips + L.x + static_cast<size_t>(cy) * L.y + cx;
-                float v = __ldg(cell);
-                if (valid_elev(v) && v > maximum_height) maximum_height = v;
-                if (has_right) {
-                    v = __ldg(cell + 1);
-                    if (valid_elev(v) && v > maximum_height) maximum_height = v;
-                }
-                if (has_down) {
-                    v = __ldg(cell + L.y);
-                    if (valid_elev(v) && v > maximum_height) maximum_height = v;
-                    if (has_right) {
-                        v = __ldg(cell + L.y + 1);
-                        if (valid_elev(v) && v > maximum_height) maximum_height = v;
-                    }
-                }
-            }
-            const float min_x = static_cast<float>(cx * scale);
-            const float min_y = static_cast<float>(cy * scale);
+            const int index = L.x + cy * L.y + cx;
+            const bool has_right = cx + 1 < L.y, has_down = cy + 1 < L.z;
+            const float v00 = __ldg(cells + index);
+            const float v10 = has_right ? __ldg(cells + index + 1) : -32000.0f;
+            const float v01 = has_down ? __ldg(cells + index + L.y) : -32000.0f;
+            const float v11 = has_right && has_down ? __ldg(cells + index + L.y + 1) : -32000.0f;
+            const float maximum_height = fmaxf(fmaxf(v00, v10), fmaxf(v01, v11));
+            const float scale_f = static_cast<float>(1 << shift);
+            const float min_x = static_cast<float>(cx << shift);
+            const float min_y = static_cast<float>(cy << shift);
             const float max_x = __fadd_rn(min_x, scale_f);
             const float max_y = __fadd_rn(min_y, scale_f);
             const float t1 = __fmul_rn(__fsub_rn(min_x, px), inv_x);
@@ -363,7 +375,7 @@ __global__ void __launch_bounds__(128) march_pass_kernel(const __grid_constant__
             const float tmx = t1 > t2 ? t1 : t2;
             const float tmy = t3 > t4 ? t3 : t4;
             const float exit_distance = tmx < tmy ? tmx : tmy;
-            const float fallback = __fmul_rn(__fmul_rn(block_m, 0.5f), 0.001f);
+            const float fallback = table.fallback[level];
             const float to_exit = exit_distance > 0.0f ? exit_distance : fallback;
             const float skip = to_exit > 0.0f ? __fadd_rn(to_exit, 0.0001f) : fallback;
             if (maximum_height < -20000.0f) {
@@ -372,22 +384,22 @@ __global__ void __launch_bounds__(128) march_pass_kernel(const __grid_constant__
             }
             float true_near = __fmaf_rn(-scale_f, resolution, true_m);
             true_near = true_near > 1.0f ? true_near : 1.0f;
-            if (bound_culled(s < 0.5f, true_near, maximum_height, radius, observer_z,
+            if (bound_culled(near, true_near, maximum_height, radius, observer_z,
                              observer_radius, inverse_denominator, current)) {
                 s = __fadd_rn(s, skip);
                 break;
             }
             if (level == 0) {
                 if (kCount) ++samples;
-                const float height = bilinear(P.level0, P.width, P.height, px, py);
+                const float height = bilinear(cells, P.width, P.height, px, py);
                 float slope = -1e30f;
-                if (valid_elev(height)) {
-                    slope = s < 0.5f ? __fdiv_rn(__fsub_rn(height, observer_z), true_m)
-                                     : sample_slope(true_m, height, radius, observer_radius);
+                if (height > -20000.0f) {
+                    slope = near ? __fdiv_rn(__fsub_rn(height, observer_z), true_m)
+                                 : sample_slope(true_m, height, radius, observer_radius);
                     if (slope > current) current = slope;
                 }
                 const float magnitude = hypot_fused(dx, dy);
-                const float pixel_step = magnitude > 1e-6f ? __fdiv_rn(1.0f, magnitude) : 0.0005f;
+                const float pixel_step = magnitude > 1e-6f ? __frcp_rn(magnitude) : 0.0005f;
                 const float margin = __fsub_rn(current, slope);
                 const float margin_step =
                     margin > 0.0f
@@ -396,7 +408,7 @@ __global__ void __launch_bounds__(128) march_pass_kernel(const __grid_constant__
                 const float angular_step = __fdiv_rn(__fmul_rn(true_m, 0.00151f), 1000.0f);
                 const float inner = margin_step < angular_step ? margin_step : angular_step;
                 float advance = pixel_step > inner ? pixel_step : inner;
-                if (s < 0.5f) advance = __fmul_rn(advance, 0.25f);
+                if (near) advance = __fmul_rn(advance, 0.25f);
                 const float floor_step =
                     (P.pass_index == 0 && true_m >= 100.0f) ? primary_far_step : minimum_step;
                 advance = advance > floor_step ? advance : floor_step;
@@ -435,19 +447,19 @@ void march_pass_device(ls200_context *ctx, const MarchTile &tile, const ls200_de
     P.azimuth_count = tile.azimuth_count;
     P.center_count = tile.center_count;
     P.dem_count = tile.dem_count;
-    P.primary_level0 = primary->level0;
+    P.primary_cells = primary->cells;
     P.primary_width = primary->width;
     P.primary_height = primary->height;
     P.primary_m6 = primary->map_parameters[6];
     P.primary_m9 = primary->map_parameters[9];
-    P.level0 = active->level0;
+    P.cells = active->cells;
     P.width = active->width;
     P.height = active->height;
-    P.mips = active->mips;
     P.level_count = active->level_count;
+    const int cells0 = active->width * active->height;
     for (int l = 0; l < active->level_count; ++l)
-        P.levels[l] = make_int4(active->levels[l].offset, active->levels[l].width,
-                                active->levels[l].height, 0);
+        P.levels[l] = make_int4(l == 0 ? 0 : cells0 + active->levels[l].offset,
+                                active->levels[l].width, active->levels[l].height, 0);
     P.m6 = active->map_parameters[6];
     P.m7 = active->map_parameters[7];
     P.m9 = active->map_parameters[9];

@@ -39,6 +39,27 @@ __global__ void __launch_bounds__(256) pyramid_downsample(const float *__restric
     destination[static_cast<size_t>(y) * width + x] = best;
 }
 
+// Invalid elevations become the -32000 block sentinel.  Every value the
+// march then reads is either valid (> -20000, finite) or exactly -32000, so
+// validity is one comparison and a four-cell bound is a plain maximum with
+// the same result as the reference's filtered maximum.
+__global__ void sanitize_kernel(const float *__restrict__ in, long long n,
+                                float *__restrict__ out) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+         i += (long long)gridDim.x * blockDim.x) {
+        const float v = in[i];
+        out[i] = valid_elevation(v) ? v : -32000.0f;
+    }
+}
+
+void sanitize_level0(ls200_context *ctx, ls200_dem *dem) {
+    const long long n = static_cast<long long>(dem->width) * dem->height;
+    const int blocks = static_cast<int>(std::min<long long>((n + 255) / 256,
+                                                            ctx->props.multiProcessorCount * 8));
+    sanitize_kernel<<<blocks, 256, 0, ctx->stream>>>(dem->level0, n, dem->cells);
+    LS_CUDA(cudaGetLastError());
+}
+
 void build_pyramid_device(ls200_context *ctx, ls200_dem *dem) {
     const float *source = dem->level0;
     int sw = dem->width, sh = dem->height;

@@ -313,6 +313,7 @@ __global__ void __launch_bounds__(128, 8) march_pass_kernel(const __grid_constan
     const float last_x = static_cast<float>(P.width - 1);
     const float last_y = static_cast<float>(P.height - 1);
     const int top_level = P.level_count - 1;
+    int level_hint = top_level;
     unsigned visits = 0, samples = 0, steps = 0;
     while (s <= s_end) {
         if (kCount) ++steps;
@@ -336,8 +337,14 @@ __global__ void __launch_bounds__(128, 8) march_pass_kernel(const __grid_constan
             true_m = __fmaf_rn(s_start_chord, 1000.0f, chord);
         }
         const float footprint = __fmul_rn(true_m, 0.004363323129985824f);
-        int level = top_level;
+        // The reference scans down from the top level to the largest level
+        // whose side fits the footprint (or 0).  Sides grow with the level,
+        // so that level is also found by moving up or down from the previous
+        // step's level, which usually takes one comparison.
+        int level = level_hint;
+        while (level < top_level && table.side[level + 1] <= footprint) ++level;
         while (level > 0 && !(table.side[level] <= footprint)) --level;
+        level_hint = level;
         // The tangent and its reciprocals depend only on delta.
         const float dx = quartic_tangent(a1, a2, a3, a4, delta);
         const float dy = quartic_tangent(b1, b2, b3, b4, delta);
@@ -363,17 +370,18 @@ __global__ void __launch_bounds__(128, 8) march_pass_kernel(const __grid_constan
             const float v01 = has_down ? __ldg(cells + index + L.y) : -32000.0f;
             const float v11 = has_right && has_down ? __ldg(cells + index + L.y + 1) : -32000.0f;
             const float maximum_height = fmaxf(fmaxf(v00, v10), fmaxf(v01, v11));
+            // Slab exit (cuda_backend.py:733-751).  Of max(t1, t2) only the
+            // far edge can win: (min_x - px) <= 0 < (max_x - px), so the
+            // product with inv_x keeps that order's sign pattern and the
+            // larger t is the edge ahead of the ray (bitwise the same value,
+            // including the -0.0 of a ray starting on the edge).
             const float scale_f = static_cast<float>(1 << shift);
             const float min_x = static_cast<float>(cx << shift);
             const float min_y = static_cast<float>(cy << shift);
-            const float max_x = __fadd_rn(min_x, scale_f);
-            const float max_y = __fadd_rn(min_y, scale_f);
-            const float t1 = __fmul_rn(__fsub_rn(min_x, px), inv_x);
-            const float t2 = __fmul_rn(__fsub_rn(max_x, px), inv_x);
-            const float t3 = __fmul_rn(__fsub_rn(min_y, py), inv_y);
-            const float t4 = __fmul_rn(__fsub_rn(max_y, py), inv_y);
-            const float tmx = t1 > t2 ? t1 : t2;
-            const float tmy = t3 > t4 ? t3 : t4;
+            const float edge_x = inv_x > 0.0f ? __fadd_rn(min_x, scale_f) : min_x;
+            const float edge_y = inv_y > 0.0f ? __fadd_rn(min_y, scale_f) : min_y;
+            const float tmx = __fmul_rn(__fsub_rn(edge_x, px), inv_x);
+            const float tmy = __fmul_rn(__fsub_rn(edge_y, py), inv_y);
             const float exit_distance = tmx < tmy ? tmx : tmy;
             const float fallback = table.fallback[level];
             const float to_exit = exit_distance > 0.0f ? exit_distance : fallback;

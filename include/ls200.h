@@ -161,6 +161,25 @@ ls200_status ls200_lighting_device(ls200_context *ctx, int tile_count, const flo
                                    const int32_t *windows, const float *horizons,
                                    const ls200_vectors *vectors, int time_start,
                                    int time_count, int signal, float *frames, void *out);
+/* Allocation-free twin of ls200_lighting_device, for callers that may not
+ * call cudaMalloc when they run (their device memory belongs to another
+ * allocator, or they cannot afford an allocation's device-wide
+ * synchronisation).  No counterpart in the reference.  Inputs and outputs
+ * are the caller's device buffers (vectors: float32[vector_count, 3]); the
+ * per-pixel frame scratch is a fixed 3 MiB device array inside this library,
+ * so tile_count is at most 4 and larger batches are rejected with
+ * LS200_ERR_INVALID.  The first call on a device looks up that array's
+ * address and uploads the disk constants; make it before any stream capture.
+ * All calls share the array: calls that overlap on the GPU (two streams, two
+ * contexts on one device) race on it.  Nothing in it needs to start at zero.
+ * Runs asynchronously on the context's stream. */
+ls200_status ls200_lighting_device_noalloc(ls200_context *ctx, int tile_count,
+                                           const float *patch_dems,
+                                           const double *geo_transforms,
+                                           const double *projections, const int32_t *windows,
+                                           const float *horizons, const float *device_vectors,
+                                           int vector_count, int time_start, int time_count,
+                                           int signal, void *out);
 /* Diagnostic: sun fraction at given (azimuth, elevation) in degrees for n
  * horizon rows float32[n,1440] (lightmap.py:32-73). */
 ls200_status ls200_sun_fraction(ls200_context *ctx, const float *horizons,

@@ -91,6 +91,8 @@ SIGNATURES: dict[str, list] = {
     "ls200_psr_run": [_vp, _vp, _vp],
     "ls200_lighting_device": [_vp, _i, _vp, _vp, _vp, _vp, _vp, _vp, _i, _i, _i, _vp, _vp],
     "ls200_sun_fraction": [_vp, _f32p, _f32p, _f32p, _i, _f32p],
+    "ls200_lighting_device_noalloc": [_vp, _i, _vp, _vp, _vp, _vp, _vp, _vp, _i, _i, _i, _i,
+                                      _vp],
     "ls200_host_alloc": [_i64, _vp],
     "ls200_host_free": [_vp],
     "ls200_fp32_probe": [_vp, _i, _vp],

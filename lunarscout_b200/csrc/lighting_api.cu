@@ -229,3 +229,93 @@ ls200_status ls200_sun_fraction(ls200_context *ctx, const float *horizons,
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// Allocation-free variant of ls200_lighting_device.
+//
+// Some callers cannot call cudaMalloc at the point where they run the
+// lighting products: a service whose device memory is owned by another
+// allocator (a framework's caching allocator, a memory pool sized at start-up)
+// may not take raw allocations, and a latency-bounded production loop cannot
+// afford cudaMalloc/cudaFree, which may synchronise the whole device.  Those
+// callers pass their own device inputs and outputs; the only working memory
+// this kernel needs beyond them, the per-pixel frame table, lives in the
+// fixed array below.
+namespace ls200 {
+
+// Scratch of the allocation-free entry point: per-pixel frames (12 floats for
+// each of the 128x128 pixels) of up to kNoAllocTiles tiles = 3 MiB.  Every GPU
+// that loads this library holds it until the process exits.
+constexpr int kNoAllocTiles = 4;
+static __device__ __align__(256) float g_noalloc_frames[size_t(kNoAllocTiles) * kPatch *
+                                                        kPatch * 12];
+
+static std::mutex g_noalloc_lock;
+static float *g_noalloc_address[64] = {};
+
+// Device address of the scratch array on the current device, looked up once
+// per device (the host-side symbol is only a stand-in for it).
+static float *noalloc_frames(int device) {
+    LS_REQUIRE(device >= 0 && device < 64, "device index out of range");
+    std::lock_guard<std::mutex> hold(g_noalloc_lock);
+    if (!g_noalloc_address[device]) {
+        void *address = nullptr;
+        const cudaError_t e = cudaGetSymbolAddress(&address, g_noalloc_frames);
+        if (e != cudaSuccess || address == nullptr)
+            throw Error(LS200_ERR_CUDA, std::string("cudaGetSymbolAddress(frame scratch): ") +
+                                            cudaGetErrorString(e));
+        g_noalloc_address[device] = static_cast<float *>(address);
+    }
+    return g_noalloc_address[device];
+}
+
+}  // namespace ls200
+
+extern "C" {
+
+ls200_status ls200_lighting_device_noalloc(ls200_context *ctx, int tile_count,
+                                           const float *patch_dems,
+                                           const double *geo_transforms,
+                                           const double *projections, const int32_t *windows,
+                                           const float *horizons, const float *device_vectors,
+                                           int vector_count, int time_start, int time_count,
+                                           int signal, void *out) {
+    return guard([&] {
+        LS_REQUIRE(ctx && patch_dems && geo_transforms && projections && windows && horizons &&
+                       device_vectors && out,
+                   "NULL argument");
+        LS_REQUIRE(tile_count >= 1 && tile_count <= kNoAllocTiles,
+                   "the allocation-free lighting entry point takes 1 to 4 tiles per call "
+                   "(its fixed frame scratch holds 4 tiles)");
+        LS_REQUIRE(signal >= kSignalFraction && signal <= kSignalPsr, "unknown signal");
+        LS_REQUIRE(vector_count > 0, "at least one vector is required");
+        LS_REQUIRE(signal == kSignalPsr ||
+                       (time_start >= 0 && time_count > 0 &&
+                        time_start + time_count <= vector_count),
+                   "time range outside the vector table");
+        std::lock_guard<std::mutex> hold(ctx->lock);
+        activate(ctx);
+        LightingBatch B{};
+        for (int t = 0; t < tile_count; ++t) {
+            std::memcpy(B.tiles[t].gt, geo_transforms + 6 * t, sizeof B.tiles[t].gt);
+            std::memcpy(B.tiles[t].proj, projections + 6 * t, sizeof B.tiles[t].proj);
+            B.tiles[t].tile_x = windows[4 * t + 0];
+            B.tiles[t].tile_y = windows[4 * t + 1];
+            B.tiles[t].valid_width = windows[4 * t + 2];
+            B.tiles[t].valid_height = windows[4 * t + 3];
+            check_valid(B.tiles[t].valid_width, B.tiles[t].valid_height);
+        }
+        B.patch_dem = patch_dems;
+        B.horizons = horizons;
+        B.vectors = device_vectors;
+        // The frames kernel writes every entry it later reads (zeros outside
+        // the valid window), so nothing in the scratch must start at zero.
+        B.frames = noalloc_frames(ctx->device);
+        B.out = out;
+        B.time_start = signal == kSignalPsr ? 0 : time_start;
+        B.time_count = signal == kSignalPsr ? vector_count : time_count;
+        lighting_launch(ctx, B, tile_count, signal);
+    });
+}
+
+}  // extern "C"

@@ -223,6 +223,108 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+LIGHT_TILES = 8
+# Per pixel x time step of the sun-fraction lightmap (lightmap_cpu.py:105-183):
+# rotate (9 mul + 9 add), radicand + sqrt, 2 atan2, 3 mul/add to degrees, bin
+# selection (6) and 16 slices of (fma-free lerp 2, add, compare/clamp 3, add,
+# fraction step 2) = about 150 FP32 operations; 1 byte written.
+LIGHT_FLOPS_PER_SAMPLE = 150
+
+
+def lighting_benchmark(session, dems, segments, tiles, primary, args, world, rank):
+    """Sun-fraction bytes for one year of hourly steps on the timed tiles'
+    horizons, computed from the device-resident march output (horizon ->
+    degrees -> lightmap on the device, no host round trip)."""
+    import ctypes
+
+    import torch
+    import torch.distributed as dist
+
+    from lunarscout_b200 import _native, synthetic
+    from lunarscout_b200.contract import projection_array
+    from lunarscout_b200.lightmap_cuda import DeviceVectors
+
+    count = min(LIGHT_TILES, args.steps)
+    picks = list(range(args.warmup, args.warmup + count))
+    plane = TILE * TILE
+    horizons = torch.empty((count, plane, AZIMUTHS), dtype=torch.float32, device="cuda")
+    patches = torch.empty((count, TILE, TILE), dtype=torch.float32, device="cuda")
+    windows = np.zeros((count, 4), dtype=np.int32)
+    elevation = torch.from_numpy(primary.elevation_m).to("cuda")
+    centers = (TILE // 8 + 2) ** 2
+    for i, k in enumerate(picks):
+        tile_row, tile_column = tiles[k]
+        session.march_all_passes_device(segments[k].data_ptr(), AZIMUTHS, centers, dems,
+                                        tile_column=tile_column, tile_row=tile_row,
+                                        observer_elevation_m=OBSERVER_M,
+                                        device_out=horizons[i].data_ptr(), degrees=True)
+        patches[i] = elevation[tile_row:tile_row + TILE, tile_column:tile_column + TILE]
+        windows[i] = (tile_column, tile_row, TILE, TILE)
+    torch.cuda.synchronize()
+    geo = np.ascontiguousarray(np.repeat(primary.geo_transform[None, :], count, 0))
+    proj = np.ascontiguousarray(np.repeat(projection_array(primary.projection)[None, :],
+                                          count, 0))
+    hours = synthetic.hours_between("2030-01-01T00", "2031-01-01T00", 1.0)
+    vectors = synthetic.sun_vectors(hours).astype(np.float32)
+    table = DeviceVectors(session.context, vectors)
+    steps = len(vectors)
+    frames = torch.empty(count * plane * 12, dtype=torch.float32, device="cuda")
+    out = torch.empty((count, steps, plane), dtype=torch.uint8, device="cuda")
+    lib = _native.library()
+
+    def launch():
+        _native.check(lib.ls200_lighting_device(
+            session.context, count, ctypes.c_void_p(patches.data_ptr()), geo.ctypes.data,
+            proj.ctypes.data, windows.ctypes.data, ctypes.c_void_p(horizons.data_ptr()),
+            table.handle, 0, steps, 1, ctypes.c_void_p(frames.data_ptr()),
+            ctypes.c_void_p(out.data_ptr())))
+
+    for _ in range(3):
+        launch()
+    torch.cuda.synchronize()
+    if world > 1:
+        dist.barrier()
+    repeats = 5
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    start.record()
+    for _ in range(repeats):
+        launch()
+    end.record()
+    torch.cuda.synchronize()
+    elapsed = start.elapsed_time(end) / 1000.0
+    if world > 1:
+        t = torch.tensor([elapsed], device="cuda", dtype=torch.float64)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        elapsed = float(t.item())
+    samples = repeats * count * plane * steps
+    value = world * samples / elapsed
+    table.close()
+    result = {
+        "metric": "lightmap px·steps/s (sun-fraction bytes, 1 year hourly)",
+        "value": value, "unit": "px·steps/s", "tiles_per_launch": count,
+        "time_steps": steps, "launches": repeats,
+        "ms_per_tile_year": 1000.0 * elapsed / (repeats * count),
+        "achieved_tflops": value * LIGHT_FLOPS_PER_SAMPLE / 1e12,
+        "output_gbs": value / 1e9,
+    }
+    if rank == 0 and world == 1 and not args.skip_cpu:
+        import oracle  # noqa: F401  (CPU leg only)
+        from oracle import products
+
+        host_horizons = horizons[0].cpu().numpy().reshape(TILE, TILE, AZIMUTHS)
+        tile_row, tile_column = tiles[picks[0]]
+        sample = vectors[:512].astype(np.float64)
+        started = time.perf_counter()
+        products.lighting_tiles(primary, host_horizons, sample, tile_y=tile_row,
+                                tile_x=tile_column)
+        took = time.perf_counter() - started
+        result["cpu_baseline"] = {
+            "value": plane * len(sample) / took, "unit": "px·steps/s",
+            "cores": products.default_threads(), "kind": "port",
+            "sample": f"one tile x {len(sample)} hourly steps ({took:.1f} s)"}
+    return result
+
+
 def run_ours(args):
     import torch
     import torch.distributed as dist
@@ -345,6 +447,8 @@ def run_ours(args):
     e2e_value = world * e2e_steps * RAYS_PER_TILE / e2e_elapsed
     e2e_session.close()
 
+    lighting = lighting_benchmark(session, dems, segments, tiles, primary, args, world, rank)
+
     fp32_peak = session.fp32_probe()
     pass_times = np.array(pass_times)
     march_seconds = float(pass_times.sum()) / (2 * args.steps)  # per launch
@@ -388,6 +492,7 @@ def run_ours(args):
             "gpu_launches": 3 * args.steps,
             "clocks": clocks,
             "segment_generation_ms_per_tile": segment_seconds * 1000.0,
+            "lightmap": lighting,
         }
         print(json.dumps(line), flush=True)
     session.close()
@@ -418,6 +523,36 @@ def run_profile_case():
                                         observer_elevation_m=OBSERVER_M,
                                         device_out=output.data_ptr())
     session.synchronize()
+    # Lighting on the same tile: one year of hourly sun-fraction bytes, twice.
+    import ctypes
+
+    from lunarscout_b200 import _native, synthetic
+    from lunarscout_b200.contract import projection_array
+    from lunarscout_b200.lightmap_cuda import DeviceVectors
+
+    session.march_all_passes_device(segments.data_ptr(), AZIMUTHS, centers, dems,
+                                    tile_column=tile_column, tile_row=tile_row,
+                                    observer_elevation_m=OBSERVER_M,
+                                    device_out=output.data_ptr(), degrees=True)
+    patch = torch.from_numpy(np.ascontiguousarray(
+        primary.elevation_m[tile_row:tile_row + TILE, tile_column:tile_column + TILE])).cuda()
+    vectors = synthetic.sun_vectors(
+        synthetic.hours_between("2030-01-01T00", "2031-01-01T00", 1.0)).astype(np.float32)
+    table = DeviceVectors(session.context, vectors)
+    frames = torch.empty(TILE * TILE * 12, dtype=torch.float32, device="cuda")
+    out = torch.empty((len(vectors), TILE * TILE), dtype=torch.uint8, device="cuda")
+    geo = np.ascontiguousarray(primary.geo_transform[None, :])
+    proj = np.ascontiguousarray(projection_array(primary.projection)[None, :])
+    window = np.array([[tile_column, tile_row, TILE, TILE]], dtype=np.int32)
+    torch.cuda.synchronize()
+    for _ in range(2):
+        _native.check(_native.library().ls200_lighting_device(
+            session.context, 1, ctypes.c_void_p(patch.data_ptr()), geo.ctypes.data,
+            proj.ctypes.data, window.ctypes.data, ctypes.c_void_p(output.data_ptr()),
+            table.handle, 0, len(vectors), 1, ctypes.c_void_p(frames.data_ptr()),
+            ctypes.c_void_p(out.data_ptr())))
+    session.synchronize()
+    table.close()
     session.close()
     log("[bench] profile case done")
 

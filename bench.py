@@ -341,7 +341,10 @@ def run_ours(args):
 
     primary, regional = build_dems()
     session = CudaSession(local)
-    stream = torch.cuda.current_stream()
+    # One explicit stream for torch and the library: the timing events are
+    # recorded on the stream the kernels are launched on.
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
     session.set_stream(stream.cuda_stream)
     dems = [session.upload_dem_grid(primary), session.upload_dem_grid(regional)]
     centers = (TILE // 8 + 2) ** 2

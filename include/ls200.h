@@ -43,9 +43,11 @@ ls200_status ls200_context_create(int device_id, ls200_context **out);
 ls200_status ls200_context_destroy(ls200_context *ctx);
 ls200_status ls200_device_info(ls200_context *ctx, char *name, int name_capacity,
                                int *major, int *minor, int *sm_count);
-/* Use `stream` (a cudaStream_t) for all later work of this context; NULL
- * restores the context's own stream. */
+/* Use `stream` (a cudaStream_t; NULL is the legacy default stream) for all
+ * later work of this context. */
 ls200_status ls200_set_stream(ls200_context *ctx, void *stream);
+/* Go back to the context's own non-blocking stream. */
+ls200_status ls200_reset_stream(ls200_context *ctx);
 ls200_status ls200_synchronize(ls200_context *ctx);
 
 /* ---- max pyramid: src/lunarscout/_numba_horizon/pyramid.py:19-31

@@ -67,6 +67,7 @@ SIGNATURES: dict[str, list] = {
     "ls200_context_destroy": [_vp],
     "ls200_device_info": [_vp, ctypes.c_char_p, _i, _vp, _vp, _vp],
     "ls200_set_stream": [_vp, _vp],
+    "ls200_reset_stream": [_vp],
     "ls200_synchronize": [_vp],
     "ls200_pyramid_layout": [_i, _i, _vp, _i, _vp, _vp],
     "ls200_build_max_pyramid": [_vp, _f32p, _i, _i, _f32p],

@@ -121,7 +121,15 @@ ls200_status ls200_set_stream(ls200_context *ctx, void *stream) {
     return guard([&] {
         LS_REQUIRE(ctx != nullptr, "context is NULL");
         std::lock_guard<std::mutex> hold(ctx->lock);
-        ctx->stream = stream ? static_cast<cudaStream_t>(stream) : ctx->own_stream;
+        ctx->stream = static_cast<cudaStream_t>(stream);  // NULL: the legacy default stream
+    });
+}
+
+ls200_status ls200_reset_stream(ls200_context *ctx) {
+    return guard([&] {
+        LS_REQUIRE(ctx != nullptr, "context is NULL");
+        std::lock_guard<std::mutex> hold(ctx->lock);
+        ctx->stream = ctx->own_stream;
     });
 }
 

@@ -112,8 +112,12 @@ class CudaSession:
         return getattr(self._production_timings, "value", None)
 
     def set_stream(self, stream_handle: int | None) -> None:
-        """Run later work on an external cudaStream_t (e.g. torch's)."""
-        call("ls200_set_stream", self._ctx, ctypes.c_void_p(stream_handle or None))
+        """Run later work on an external cudaStream_t (e.g. torch's; 0 is the
+        legacy default stream); None goes back to the session's own stream."""
+        if stream_handle is None:
+            call("ls200_reset_stream", self._ctx)
+        else:
+            call("ls200_set_stream", self._ctx, ctypes.c_void_p(stream_handle))
 
     def synchronize(self) -> None:
         call("ls200_synchronize", self._ctx)

@@ -61,6 +61,18 @@ def log(*args):
     print(*args, file=sys.stderr, flush=True)
 
 
+def profiled_traffic(name: str):
+    """DRAM bytes per launch recorded by the committed ncu summary, if any."""
+    path = ROOT / "profiles" / name
+    try:
+        for line in path.read_text().splitlines():
+            if line.startswith("dram_bytes_per_launch:"):
+                return int(line.split(":", 1)[1])
+    except OSError:
+        return None
+    return None
+
+
 def dist_env():
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -313,7 +325,7 @@ def lighting_benchmark(session, dems, segments, tiles, primary, args, world, ran
 
         host_horizons = horizons[0].cpu().numpy().reshape(TILE, TILE, AZIMUTHS)
         tile_row, tile_column = tiles[picks[0]]
-        sample = vectors[:512].astype(np.float64)
+        sample = vectors.astype(np.float64)  # one tile, the whole year
         started = time.perf_counter()
         products.lighting_tiles(primary, host_horizons, sample, tile_y=tile_row,
                                 tile_x=tile_column)
@@ -481,7 +493,9 @@ def run_ours(args):
                 "frac": achieved / fp32_peak,
                 "peak_source": "FP32 FMA probe measured in this run (no FP32 entry in "
                                "MEASURED_PEAKS.json)",
-                "traffic": None,
+                "traffic": profiled_traffic("march_pass_kernel_site_tile.md"),
+                "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one "
+                                  "pass-0 launch (profiles/march_pass_kernel_site_tile.md)",
                 "algorithmic_flops_per_launch": flops,
                 "gathered_bytes_per_launch": gathered,
                 "launch_ms": march_seconds * 1000.0,

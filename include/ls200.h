@@ -125,10 +125,39 @@ ls200_status ls200_set_counting(ls200_context *ctx, int enabled);
 ls200_status ls200_last_counters(ls200_context *ctx, int64_t *visits, int64_t *samples,
                                  int64_t *steps);
 
+/* One horizon tile end to end on the device, the work of one patch of
+ * src/lunarscout/horizon.py:137-238 (_run_horizon_pipeline: prepare =
+ * build_subpatch_segments_numba, process = generate_patch_horizons, finalize
+ * = HorizonBuffers.degrees, then the .cbin encoder): segments, every DEM
+ * pass, degrees, and with `compress` the .cbin payload.  Pixels outside the
+ * primary DEM (partial right/bottom tiles) hold -50 degrees, as the
+ * reference's writer pads them (file_format.py:93-120).  `out` (host) gets
+ * the payload (capacity >= 16384*2882) or raw pixel-major float32 degrees
+ * (capacity >= 16384*azimuth_count*4); *size the byte count. */
+ls200_status ls200_horizon_tile(ls200_context *ctx, ls200_dem *const *dems, int dem_count,
+                                int tile_column, int tile_row, int azimuth_count,
+                                double maximum_distance_m, float observer_elevation_m,
+                                int subpatch_size, int compress, void *out, int64_t capacity,
+                                int64_t *size);
+
 /* slope -> degrees, float32(atan(s) * float32(180/pi)), -inf preserved:
  * src/lunarscout/_numba_horizon/contract.py:362-371 (HorizonBuffers.degrees) */
 ls200_status ls200_slopes_to_degrees(ls200_context *ctx, const float *slopes, int64_t count,
                                      float *degrees);
+
+/* ---- horizon tile codec (.cbin): src/lunarscout/_numba_horizon/file_format.py:39-73
+ *      (_encode_horizons_python) and :135-182 (_decode_compressed_payload_into_python) ---- */
+/* Pixel-major degrees float32[16384*1440] (host) -> payload (host, capacity
+ * >= 16384*2882 bytes); *size receives the payload length. */
+ls200_status ls200_cbin_encode(ls200_context *ctx, const float *degrees, uint8_t *payload,
+                               int64_t capacity, int64_t *size);
+/* The same on device buffers (payload capacity >= 16384*2882 bytes). */
+ls200_status ls200_cbin_encode_device(ls200_context *ctx, const float *device_degrees,
+                                      uint8_t *device_payload, int64_t *size);
+/* Payload (host) -> degrees float32[16384*1440] (host); LS200_ERR_INVALID for
+ * a structurally invalid payload. */
+ls200_status ls200_cbin_decode(ls200_context *ctx, const uint8_t *payload, int64_t size,
+                               float *degrees);
 
 /* ---- lighting products: src/lunarscout/_numba_horizon/lightmap_cuda.py:187-276
  *      (LightmapCudaSession) and psr_cuda.py:191-375 (PsrCudaSession) ---- */

@@ -96,6 +96,7 @@ ls200_status ls200_context_destroy(ls200_context *ctx) {
         }
         ctx->dems.clear();
         release_lighting_state(ctx);
+        release_codec(ctx);
         for (auto &event : ctx->events)
             if (event) cudaEventDestroy(event);
         if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);

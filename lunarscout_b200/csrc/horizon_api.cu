@@ -58,6 +58,17 @@ __global__ void degrees_kernel(const float *__restrict__ in, int64_t n, float *_
     }
 }
 
+// Pixels of a 128x128 pixel-major tile outside the valid (DEM-covered)
+// rectangle become -50 degrees, the codec's minimum (file_format.py:93-120).
+__global__ void pad_outside_kernel(float *__restrict__ tile, int valid_width, int valid_height,
+                                   int azimuth_count) {
+    const int pixel = blockIdx.x;
+    const int row = pixel / 128, column = pixel % 128;
+    if (row < valid_height && column < valid_width) return;
+    float *out = tile + static_cast<size_t>(pixel) * azimuth_count;
+    for (int a = threadIdx.x; a < azimuth_count; a += blockDim.x) out[a] = -50.0f;
+}
+
 void slopes_to_degrees_device(ls200_context *ctx, const float *slopes, int64_t count,
                               float *degrees) {
     const int blocks = static_cast<int>(std::min<int64_t>((count + 255) / 256,
@@ -223,6 +234,59 @@ ls200_status ls200_march_all_passes_device(ls200_context *ctx, const float *devi
                        tile_column, tile_row, tile_width, tile_height, subpatch_size,
                        observer_elevation_m};
         all_passes_device(ctx, tile, dems, device_out, degrees != 0, pass_seconds);
+    });
+}
+
+ls200_status ls200_horizon_tile(ls200_context *ctx, ls200_dem *const *dems, int dem_count,
+                                int tile_column, int tile_row, int azimuth_count,
+                                double maximum_distance_m, float observer_elevation_m,
+                                int subpatch_size, int compress, void *out, int64_t capacity,
+                                int64_t *size) {
+    return guard([&] {
+        LS_REQUIRE(ctx && dems && out && size && dem_count > 0, "NULL argument");
+        for (int d = 0; d < dem_count; ++d) LS_REQUIRE(dems[d] != nullptr, "NULL DEM");
+        LS_REQUIRE(azimuth_count == 1440 || !compress,
+                   "the .cbin tile format holds exactly 1440 azimuths");
+        const int tile = 128;
+        const int count = tile / subpatch_size + 2;
+        check_tile(azimuth_count, count * count, dem_count, tile, tile, subpatch_size);
+        const size_t samples = size_t(tile) * tile * azimuth_count;
+        const size_t max_payload = size_t(tile) * tile * (2 * 1440 + 2);
+        LS_REQUIRE(capacity >= int64_t(compress ? max_payload : samples * sizeof(float)),
+                   "output capacity is too small for one tile");
+        LS_REQUIRE(tile_column >= 0 && tile_row >= 0, "tile origin must be non-negative");
+        const int valid_width = std::min(tile, dems[0]->width - tile_column);
+        const int valid_height = std::min(tile, dems[0]->height - tile_row);
+        LS_REQUIRE(valid_width > 0 && valid_height > 0, "tile origin lies outside the primary DEM");
+        std::unique_lock<std::mutex> hold(ctx->lock);
+        activate(ctx);
+        const size_t seg_bytes =
+            sizeof(float) * size_t(azimuth_count) * count * count * dem_count * kSegmentFields;
+        ctx->segments.reserve(seg_bytes);
+        ctx->output.reserve(samples * sizeof(float));
+        segments_device(ctx, dems, dem_count, tile_column, tile_row, tile, azimuth_count,
+                        maximum_distance_m, observer_elevation_m, subpatch_size,
+                        ctx->segments.as<float>());
+        MarchTile mt{ctx->segments.as<float>(), azimuth_count, count * count, dem_count,
+                     tile_column, tile_row, tile, tile, subpatch_size, observer_elevation_m};
+        all_passes_device(ctx, mt, dems, ctx->output.as<float>(), true, nullptr);
+        if (valid_width < tile || valid_height < tile) {
+            pad_outside_kernel<<<tile * tile, 256, 0, ctx->stream>>>(
+                ctx->output.as<float>(), valid_width, valid_height, azimuth_count);
+            LS_CUDA(cudaGetLastError());
+        }
+        if (compress) {
+            ctx->scratch.reserve(max_payload);
+            const int64_t n = cbin_encode(ctx, ctx->output.as<float>(), ctx->scratch.as<uint8_t>());
+            LS_CUDA(cudaMemcpyAsync(out, ctx->scratch.ptr, size_t(n), cudaMemcpyDeviceToHost,
+                                    ctx->stream));
+            *size = n;
+        } else {
+            LS_CUDA(cudaMemcpyAsync(out, ctx->output.ptr, samples * sizeof(float),
+                                    cudaMemcpyDeviceToHost, ctx->stream));
+            *size = int64_t(samples * sizeof(float));
+        }
+        LS_CUDA(cudaStreamSynchronize(ctx->stream));
     });
 }
 

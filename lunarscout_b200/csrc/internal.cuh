@@ -86,6 +86,7 @@ struct PyramidLevel {
 };
 
 struct LightingState;  // lighting tile buffers of a context (lighting_api.cu)
+struct CodecBuffers;   // .cbin codec buffers of a context (codec.cu)
 
 }  // namespace ls200
 
@@ -121,6 +122,7 @@ struct ls200_context {
     cudaEvent_t events[ls200::kMaxLevels + 2] = {};
     std::set<ls200_dem *> dems;  // live DEMs, released with the context
     ls200::LightingState *lighting = nullptr;
+    ls200::CodecBuffers *codec = nullptr;
 };
 
 namespace ls200 {
@@ -130,6 +132,11 @@ void activate(ls200_context *ctx);
 
 // Free the lighting buffers and vector tables owned by a context.
 void release_lighting_state(ls200_context *ctx);
+// Free the codec buffers owned by a context.
+void release_codec(ls200_context *ctx);
+// .cbin-encode device degrees [16384, 1440] into device `payload` (capacity
+// >= 16384 * 2882 bytes) on ctx->stream; returns the size (synchronises).
+int64_t cbin_encode(ls200_context *ctx, const float *degrees, uint8_t *payload);
 
 int pyramid_layout(int width, int height, PyramidLevel *levels, int capacity,
                    int64_t *mip_count);

@@ -140,6 +140,30 @@ ls200_status ls200_horizon_tile(ls200_context *ctx, ls200_dem *const *dems, int 
                                 int subpatch_size, int compress, void *out, int64_t capacity,
                                 int64_t *size);
 
+/* One 128x128 tile of one site in a multi-site batch. */
+typedef struct ls200_site_tile {
+    ls200_dem *const *dems;     /* the site's DEMs in pass order, primary first (1..8) */
+    int dem_count;
+    int tile_column, tile_row;  /* tile origin in primary-DEM pixels */
+    double maximum_distance_m;  /* ray range (the public path uses 1,000 km) */
+    float observer_elevation_m;
+} ls200_site_tile;
+
+/* Batched persistent march, no single reference counterpart: the work of
+ * generate_patch_horizons (src/lunarscout/_numba_horizon/generator.py:11-40)
+ * for `tile_count` tiles of any sites in one launch.  Segments are built on
+ * the device per tile, then one resident grid marches every (tile, pixel,
+ * azimuth) ray through all of its tile's DEM passes with work stealing.
+ * traversal 0: the reference traversal, bit-identical to ls200_march_all_passes;
+ * traversal 1: the skip ladder (a cull extends to the largest culled ancestor
+ * cell, from 1 km on).  `device_out` holds tile_count x 16384 x azimuth_count
+ * floats, pixel-major per tile: slopes, or degrees when `degrees` (-inf kept
+ * outside the primary DEM).  `seconds` (may be NULL) gets
+ * {segments + setup, march}. */
+ls200_status ls200_march_sites(ls200_context *ctx, const ls200_site_tile *tiles, int tile_count,
+                               int azimuth_count, int subpatch_size, int traversal,
+                               int degrees, void *device_out, double *seconds);
+
 /* slope -> degrees, float32(atan(s) * float32(180/pi)), -inf preserved:
  * src/lunarscout/_numba_horizon/contract.py:362-371 (HorizonBuffers.degrees) */
 ls200_status ls200_slopes_to_degrees(ls200_context *ctx, const float *slopes, int64_t count,

@@ -86,6 +86,7 @@ SIGNATURES: dict[str, list] = {
     "ls200_last_counters": [_vp, _vp, _vp, _vp],
     "ls200_slopes_to_degrees": [_vp, _f32p, _i64, _f32p],
     "ls200_horizon_tile": [_vp, _vp, _i, _i, _i, _i, _d, _f, _i, _i, _vp, _i64, _vp],
+    "ls200_march_sites": [_vp, _vp, _i, _i, _i, _i, _i, _vp, _vp],
     "ls200_cbin_encode": [_vp, _f32p, _vp, _i64, _vp],
     "ls200_cbin_encode_device": [_vp, _vp, _vp, _vp],
     "ls200_cbin_decode": [_vp, _vp, _i64, _f32p],

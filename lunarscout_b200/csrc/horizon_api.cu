@@ -5,10 +5,6 @@
 
 namespace ls200 {
 
-// float32(180) / float32(pi) evaluated in float32, the factor of
-// HorizonBuffers.degrees (one ulp below float32(180/pi)).
-constexpr float kSlopeDegrees = 0x1.ca5dcp+5f;
-
 // az-major [A, P] -> pixel-major [P, A] through a 32x32 shared tile; with
 // `degrees` the value is float32(atanf(s) * float32(180/pi)) and -inf stays
 // -inf (contract.py:362-371).
@@ -92,7 +88,7 @@ static void check_tile(int azimuth_count, int center_count, int dem_count, int t
                "tile exceeds the int32 thread index range");
 }
 
-static void resolve_counters(ls200_context *ctx) {
+void resolve_counters(ls200_context *ctx) {
     if (!ctx->counting) return;
     unsigned long long host[3] = {0, 0, 0};
     LS_CUDA(cudaMemcpyAsync(host, ctx->counters.ptr, sizeof host, cudaMemcpyDeviceToHost,
@@ -103,7 +99,7 @@ static void resolve_counters(ls200_context *ctx) {
     ctx->last_steps = host[2];
 }
 
-static void reset_counters(ls200_context *ctx) {
+void reset_counters(ls200_context *ctx) {
     if (ctx->counting)
         LS_CUDA(cudaMemsetAsync(ctx->counters.ptr, 0, 3 * sizeof(unsigned long long),
                                 ctx->stream));

@@ -19,6 +19,10 @@ constexpr int kMaxLevels = 20;   // 4^19 cells per side is far beyond any DEM
 constexpr int kSegmentFields = 18;
 constexpr int kMarchFields = 16;  // fields 0,1,4..17 of a segment
 
+// float32(180) / float32(pi) evaluated in float32, the factor of
+// HorizonBuffers.degrees (one ulp below float32(180/pi)).
+constexpr float kSlopeDegrees = 0x1.ca5dcp+5f;
+
 // An error carrying the status it maps to at the C boundary.
 struct Error : std::runtime_error {
     ls200_status status;
@@ -164,6 +168,11 @@ struct MarchTile {
 void march_pass_device(ls200_context *ctx, const MarchTile &tile, const ls200_dem *primary,
                        const ls200_dem *active, int pass_index, bool first_pass,
                        float *slopes_az_major);
+
+// Zero the march counters before a counted launch / read them back after it
+// (both no-ops unless counting is enabled).
+void reset_counters(ls200_context *ctx);
+void resolve_counters(ls200_context *ctx);
 
 // az-major [A, P] -> pixel-major [P, A], optionally as degrees.
 void transpose_slopes(ls200_context *ctx, const float *az_major, int azimuth_count,

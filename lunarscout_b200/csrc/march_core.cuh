@@ -1,0 +1,491 @@
+// The per-ray core of the horizon march, shared by the per-tile production
+// kernel (march.cu) and the persistent multi-site kernel (march_batch.cu).
+//
+// Semantics follow src/lunarscout/_numba_horizon/cuda_backend.py:
+//   subpatch_hierarchy_kernel :1007-1134 (segment interpolation, observer)
+//   hierarchy_maximum          :656-874  (the march)
+//   helpers                    :43-132
+//
+// Arithmetic contract.  The including files are compiled with --fmad=false,
+// so every written multiply and add rounds separately, and the multiply-adds
+// that the reference's GPU compiler fuses are written as explicit __fmaf_rn:
+//   * every "x + a*b" / "x - a*b" whose product feeds the add is fused;
+//   * for "a*b + c*d" the first product is fused.
+// Division, reciprocal and square root are IEEE round-to-nearest.  With the
+// same segment inputs the results are bit-identical to the CPU oracle's FP32
+// restatement, which reproduces the reference's golden traversal captures.
+//
+// The march is bound by instruction issue (its gathers hit L1/L2), so the
+// work per node visit is kept small without changing any rounded value or
+// decision:
+//   * cells come from a sanitized copy of level 0 (invalid -> -32000) packed
+//     with the mips, so validity is one comparison and the four-cell bound
+//     is a plain maximum;
+//   * per-level constants (cell side, step and fallback advances, offsets)
+//     come from a table computed once per DEM;
+//   * the tangent and its reciprocals depend only on the ray position and are
+//     computed once per position, not per level;
+//   * the cull test decides with a cheap bound outside a guard band and with
+//     the reference arithmetic inside it (bound_culled).
+//
+// The skip ladder (kLadder, the batched traversal; no reference counterpart)
+// extends a cull to the largest culled ancestor cell, see ladder_advance.
+#pragma once
+
+#include "internal.cuh"
+
+namespace ls200 {
+
+// Per-level constants of one DEM.
+struct LevelTable {
+    float side[kMaxLevels];      // float(4^l) * resolution: the level choice
+    float fallback[kMaxLevels];  // ((side * 0.5) * 0.001)
+    float out_step[kMaxLevels];  // max(0.001, side * 0.001)
+    int4 cells[kMaxLevels];      // (cell offset, width, height, -)
+};
+
+// Everything the march of one DEM pass needs about the DEM.
+struct DemView {
+    const float *cells;  // sanitized level 0 + packed mips
+    int width, height, level_count;
+    float resolution;    // mean pixel size of the DEM (m)
+    float column_res;    // hypot of the column axis of the geotransform
+    float radius;
+};
+
+// The ladder acts from this distance on (m); nearer, steep crater walls make
+// the reference's slope formula sensitive to where samples fall.
+constexpr float kLadderMinimumDistance = 1000.0f;
+
+// Warp-aggregated counter update over the lanes that reach it together
+// (counting launches are diagnostics, never timed).
+__device__ __forceinline__ void add_counters(unsigned long long *counters, unsigned visits,
+                                             unsigned samples, unsigned steps) {
+    const unsigned mask = __activemask();
+    const unsigned v = __reduce_add_sync(mask, visits);
+    const unsigned n = __reduce_add_sync(mask, samples);
+    const unsigned t = __reduce_add_sync(mask, steps);
+    if ((threadIdx.x & 31) == __ffs(mask) - 1) {
+        atomicAdd(counters, static_cast<unsigned long long>(v));
+        atomicAdd(counters + 1, static_cast<unsigned long long>(n));
+        atomicAdd(counters + 2, static_cast<unsigned long long>(t));
+    }
+}
+
+__device__ __forceinline__ float hypot_fused(float a, float b) {
+    return __fsqrt_rn(__fmaf_rn(a, a, __fmul_rn(b, b)));
+}
+
+// Mean pixel size (m) from the geotransform terms m6, m7 (column axis) and
+// m9, m10 (row axis) (cuda_backend.py:1036-1040).
+__device__ __forceinline__ float mean_resolution(float m6, float m7, float m9, float m10) {
+    return __fmul_rn(__fadd_rn(hypot_fused(m6, m9), hypot_fused(m7, m10)), 0.5f);
+}
+
+// Fill entry `l` of a level table (block_m = float(4^l) * resolution).
+__device__ __forceinline__ void fill_level(LevelTable &table, int l, float resolution,
+                                           int4 cells) {
+    const float block_m = __fmul_rn(static_cast<float>(1 << (2 * l)), resolution);
+    const float step_km = __fmul_rn(block_m, 0.001f);
+    table.side[l] = block_m;
+    table.fallback[l] = __fmul_rn(__fmul_rn(block_m, 0.5f), 0.001f);
+    table.out_step[l] = 0.001f > step_km ? 0.001f : step_km;
+    table.cells[l] = cells;
+}
+
+__device__ __forceinline__ float quartic(float x0, float a1, float a2, float a3, float a4,
+                                         float d) {
+    const float d2 = __fmul_rn(d, d);
+    const float d3 = __fmul_rn(d2, d);
+    const float d4 = __fmul_rn(d2, d2);
+    float r = __fmaf_rn(a1, d, x0);
+    r = __fmaf_rn(a2, d2, r);
+    r = __fmaf_rn(a3, d3, r);
+    return __fmaf_rn(a4, d4, r);
+}
+
+__device__ __forceinline__ float quartic_tangent(float a1, float a2, float a3, float a4,
+                                                 float d) {
+    const float d2 = __fmul_rn(d, d);
+    const float d3 = __fmul_rn(d2, d);
+    float r = __fmaf_rn(__fmul_rn(2.0f, a2), d, a1);
+    r = __fmaf_rn(__fmul_rn(3.0f, a3), d2, r);
+    return __fmaf_rn(__fmul_rn(4.0f, a4), d3, r);
+}
+
+// Clamped bilinear sample of sanitized level-0 cells; -32000 when any corner
+// is invalid (cuda_backend.py:107-132).
+__device__ __forceinline__ float bilinear(const float *__restrict__ cells, int width,
+                                          int height, float column, float row) {
+    const float cmax = __fsub_rn(static_cast<float>(width), 1.0001f);
+    const float rmax = __fsub_rn(static_cast<float>(height), 1.0001f);
+    column = column > 0.0f ? column : 0.0f;
+    column = column < cmax ? column : cmax;
+    row = row > 0.0f ? row : 0.0f;
+    row = row < rmax ? row : rmax;
+    const int x0 = static_cast<int>(floorf(column));
+    const int y0 = static_cast<int>(floorf(row));
+    const int x1 = min(x0 + 1, width - 1);
+    const int y1 = min(y0 + 1, height - 1);
+    const float *r0 = cells + static_cast<size_t>(y0) * width;
+    const float *r1 = cells + static_cast<size_t>(y1) * width;
+    const float q00 = __ldg(r0 + x0), q10 = __ldg(r0 + x1);
+    const float q01 = __ldg(r1 + x0), q11 = __ldg(r1 + x1);
+    if (!(q00 > -20000.0f && q10 > -20000.0f && q01 > -20000.0f && q11 > -20000.0f))
+        return -32000.0f;
+    const float tx = __fsub_rn(column, static_cast<float>(x0));
+    const float ty = __fsub_rn(row, static_cast<float>(y0));
+    const float top = __fmaf_rn(tx, __fsub_rn(q10, q00), q00);
+    const float bottom = __fmaf_rn(tx, __fsub_rn(q11, q01), q01);
+    return __fmaf_rn(ty, __fsub_rn(bottom, top), top);
+}
+
+// Local-z slope of a terrain point seen over the chord `dist`
+// (cuda_backend.py:812-830): numerator fused on its first product, local_x^2
+// fused on dist*dist.
+__device__ __forceinline__ float sample_slope(float dist, float height, float radius,
+                                              float observer_radius) {
+    const float squared = __fmul_rn(dist, dist);
+    const float point_radius = __fadd_rn(radius, height);
+    const float radius_delta = __fsub_rn(point_radius, observer_radius);
+    const float radius_sum = __fadd_rn(point_radius, observer_radius);
+    const float numerator = __fmaf_rn(radius_delta, radius_sum, -squared);
+    const float local_z = __fdiv_rn(numerator, __fmul_rn(2.0f, observer_radius));
+    const float lx2 = __fmaf_rn(dist, dist, -__fmul_rn(local_z, local_z));
+    const float local_x = lx2 > 0.0f ? __fsqrt_rn(lx2) : 1e-6f;
+    return __fdiv_rn(local_z, local_x);
+}
+
+// The same for the four-cell culling bound (cuda_backend.py:777-795).
+__device__ __forceinline__ float bound_slope(float dist, float height, float radius,
+                                             float observer_z, float observer_radius) {
+    const float squared = __fmul_rn(dist, dist);
+    const float height_delta = __fsub_rn(height, observer_z);
+    float radius_sum = __fadd_rn(__fmul_rn(2.0f, radius), height);
+    radius_sum = __fadd_rn(radius_sum, observer_z);
+    const float numerator = __fmaf_rn(height_delta, radius_sum, -squared);
+    const float local_z = __fdiv_rn(numerator, __fmul_rn(2.0f, observer_radius));
+    const float lx2 = __fmaf_rn(dist, dist, -__fmul_rn(local_z, local_z));
+    const float local_x = lx2 > 0.0f ? __fsqrt_rn(lx2) : 1e-6f;
+    return __fdiv_rn(local_z, local_x);
+}
+
+// Exactly `possible <= current` for the four-cell bound `possible` of the
+// reference (near field: fl((h - oz) / tn); far field: bound_slope), at a
+// fraction of its cost.  The cull test is the most frequent operation of the
+// march and `possible` only feeds this comparison, so an approximation may
+// decide it whenever it lies outside a guard band around `current`:
+//   near: __fdividef has at most 2 ulp error;
+//   far:  the numerator is the exact one; z = num * rcp(den) is within 3 ulp
+//         of fl(num / den); with local_x^2 > tn^2 / 4 (bound below 60 deg)
+//         the cancellation in local_x^2 amplifies that by at most 3, and
+//         rsqrtf adds 2 ulp: the approximation is within 2e-6 (relative) of
+//         the exact FP32 value.
+// The band is 1e-5 relative, five times that bound; inside it, and for
+// steeper bounds, the exact arithmetic of the reference decides.
+__device__ __forceinline__ bool bound_culled(bool near, float true_near, float height,
+                                             float radius, float observer_z,
+                                             float observer_radius, float inverse_denominator,
+                                             float current) {
+    float approx;
+    if (near) {
+        approx = __fdividef(__fsub_rn(height, observer_z), true_near);
+    } else {
+        const float squared = __fmul_rn(true_near, true_near);
+        const float height_delta = __fsub_rn(height, observer_z);
+        float radius_sum = __fadd_rn(__fmul_rn(2.0f, radius), height);
+        radius_sum = __fadd_rn(radius_sum, observer_z);
+        const float numerator = __fmaf_rn(height_delta, radius_sum, -squared);
+        const float local_z = __fmul_rn(numerator, inverse_denominator);
+        const float lx2 = __fmaf_rn(true_near, true_near, -__fmul_rn(local_z, local_z));
+        if (!(lx2 > 0.25f * squared)) {
+            return bound_slope(true_near, height, radius, observer_z, observer_radius) <= current;
+        }
+        approx = __fmul_rn(local_z, rsqrtf(lx2));
+    }
+    const float band = 1e-5f * fmaxf(fabsf(approx), fabsf(current));
+    if (approx < current - band) return true;
+    if (approx > current + band) return false;
+    const float possible =
+        near ? __fdiv_rn(__fsub_rn(height, observer_z), true_near)
+             : bound_slope(true_near, height, radius, observer_z, observer_radius);
+    return possible <= current;
+}
+
+__device__ __forceinline__ int clamp_center(int requested, int dem_size, int subpatch) {
+    const int half = subpatch / 2;
+    int maximum = dem_size - half;
+    if (maximum < half) maximum = half;
+    if (requested < half) return half;
+    if (requested > maximum) return maximum;
+    return requested;
+}
+
+// Four-cell bound of the level cell (cx, cy): the maximum of the cell and its
+// right / lower / diagonal neighbours, -32000 standing in for a missing one.
+__device__ __forceinline__ float four_cell_bound(const float *__restrict__ cells, int4 L,
+                                                 int cx, int cy) {
+    const int index = L.x + cy * L.y + cx;
+    const bool has_right = cx + 1 < L.y, has_down = cy + 1 < L.z;
+    const float v00 = __ldg(cells + index);
+    const float v10 = has_right ? __ldg(cells + index + 1) : -32000.0f;
+    const float v01 = has_down ? __ldg(cells + index + L.y) : -32000.0f;
+    const float v11 = has_right && has_down ? __ldg(cells + index + L.y + 1) : -32000.0f;
+    return fmaxf(fmaxf(v00, v10), fmaxf(v01, v11));
+}
+
+// Advance (km) to the exit of the cell (cx, cy) of side 4^level pixels along
+// the tangent, + 1e-4 km, or `fallback` when the exit is not ahead
+// (cuda_backend.py:733-762).  Of max(t1, t2) only the far edge can win:
+// (min_x - px) <= 0 < (max_x - px), so the product with inv_x keeps that
+// order's sign pattern and the larger t is the edge ahead of the ray
+// (bitwise the same value, including the -0.0 of a ray starting on the edge).
+__device__ __forceinline__ float cell_exit_advance(int shift, int cx, int cy, float px, float py,
+                                                   float inv_x, float inv_y, float fallback) {
+    const float scale_f = static_cast<float>(1 << shift);
+    const float min_x = static_cast<float>(cx << shift);
+    const float min_y = static_cast<float>(cy << shift);
+    const float edge_x = inv_x > 0.0f ? __fadd_rn(min_x, scale_f) : min_x;
+    const float edge_y = inv_y > 0.0f ? __fadd_rn(min_y, scale_f) : min_y;
+    const float tmx = __fmul_rn(__fsub_rn(edge_x, px), inv_x);
+    const float tmy = __fmul_rn(__fsub_rn(edge_y, py), inv_y);
+    const float exit_distance = tmx < tmy ? tmx : tmy;
+    const float to_exit = exit_distance > 0.0f ? exit_distance : fallback;
+    return to_exit > 0.0f ? __fadd_rn(to_exit, 0.0001f) : fallback;
+}
+
+// The skip ladder.  After a cull at `level`, climb to the ancestors of the
+// cell while each is culled by a conservative test, and return the advance
+// to the exit of the largest culled one (`advance` when none is).  Every
+// ancestor of an in-range cell is in range.  The test bounds the slope of
+// every sample the skip passes over: heights are <= the ancestor's four-cell
+// bound h, distances lie in [d0, d1] with d0 = true_m (distance grows along
+// the ray) and d1 = d0 + 1010 m per km of advance + 1 m (a chord never
+// outgrows the path).  With dh = h - observer_z >= 0 the slope falls with
+// distance, so the bound is the slope formula at d0; with dh < 0 every slope
+// is below dh / d1 (the curvature drop only lowers it).  The cull needs the
+// bound below `current` by a relative 4e-6, which covers its rounding.
+template <bool kCount, class Table>
+__device__ __forceinline__ float ladder_advance(const Table &table, const float *__restrict__ cells,
+                                                int level, int top, int ipx, int ipy, float px,
+                                                float py, float inv_x, float inv_y, bool near,
+                                                float true_m, float radius, float observer_z,
+                                                float observer_radius, float current,
+                                                float advance, unsigned &visits) {
+    if (true_m < kLadderMinimumDistance) return advance;
+    float best = advance;
+    for (int m = level + 1; m <= top; ++m) {
+        const int shift = 2 * m;
+        const int cx = ipx >> shift, cy = ipy >> shift;
+        const float maximum_height = four_cell_bound(cells, table.cells(m), cx, cy);
+        const float step =
+            cell_exit_advance(shift, cx, cy, px, py, inv_x, inv_y, table.fallback(m));
+        if (kCount) ++visits;
+        if (!(maximum_height < -20000.0f)) {
+            const float dh = __fsub_rn(maximum_height, observer_z);
+            float bound;
+            if (dh >= 0.0f) {
+                bound = near ? __fdiv_rn(dh, true_m)
+                             : bound_slope(true_m, maximum_height, radius, observer_z,
+                                           observer_radius);
+            } else {
+                bound = __fdiv_rn(dh, __fadd_rn(__fadd_rn(true_m, __fmul_rn(step, 1010.0f)), 1.0f));
+            }
+            const float size = fmaxf(fabsf(bound), fabsf(current));
+            if (!(__fadd_rn(bound, __fmul_rn(4e-6f, size)) <= current)) break;
+        }
+        best = step;
+    }
+    return best;
+}
+
+// One interpolated segment (fields 0,1,4..17 of the reference layout).
+struct RaySegment {
+    float start_x, start_y, a1, a2, a3, a4, b1, b2, b3, b4;
+    float s_start, s_end, s_start_chord, c1, c2, c3;
+};
+
+// Subpatch interpolation of one ray's segment (cuda_backend.py:1032-1119):
+// four centres around the pixel, their start points shifted to the pixel.
+__device__ __forceinline__ RaySegment interpolate_segment(
+    const float *__restrict__ segments, int center_count, int dem_count, int pass_index,
+    int azimuth, int column, int row, int tile_column, int tile_row, int tile_width,
+    int subpatch, int primary_width, int primary_height, float ratio) {
+    const int count = tile_width / subpatch + 2;
+    const float gx = __fadd_rn(__fdiv_rn(static_cast<float>(column - subpatch / 2),
+                                         static_cast<float>(subpatch)), 1.0f);
+    const float gy = __fadd_rn(__fdiv_rn(static_cast<float>(row - subpatch / 2),
+                                         static_cast<float>(subpatch)), 1.0f);
+    int left = static_cast<int>(gx), top = static_cast<int>(gy);
+    float tx = __fsub_rn(gx, static_cast<float>(left));
+    float ty = __fsub_rn(gy, static_cast<float>(top));
+    if (left < 0) { left = 0; tx = 0.0f; }
+    if (top < 0) { top = 0; ty = 0.0f; }
+    if (left > count - 2) { left = count - 2; tx = 1.0f; }
+    if (top > count - 2) { top = count - 2; ty = 1.0f; }
+    const int i00 = top * count + left, i10 = i00 + 1;
+    const int i01 = (top + 1) * count + left, i11 = i01 + 1;
+    const int req_left = tile_column + (left - 1) * subpatch + subpatch / 2;
+    const int req_top = tile_row + (top - 1) * subpatch + subpatch / 2;
+    const float d_left = static_cast<float>(
+        column - (clamp_center(req_left, primary_width, subpatch) - tile_column));
+    const float d_right = static_cast<float>(
+        column - (clamp_center(req_left + subpatch, primary_width, subpatch) - tile_column));
+    const float d_top = static_cast<float>(
+        row - (clamp_center(req_top, primary_height, subpatch) - tile_row));
+    const float d_bottom = static_cast<float>(
+        row - (clamp_center(req_top + subpatch, primary_height, subpatch) - tile_row));
+
+    const size_t stride_c = static_cast<size_t>(dem_count) * kSegmentFields;
+    const float *base = segments + static_cast<size_t>(azimuth) * center_count * stride_c +
+                        static_cast<size_t>(pass_index) * kSegmentFields;
+    const float *s00 = base + i00 * stride_c, *s10 = base + i10 * stride_c;
+    const float *s01 = base + i01 * stride_c, *s11 = base + i11 * stride_c;
+    float seg[kMarchFields];
+#pragma unroll
+    for (int k = 0; k < kMarchFields; ++k) {
+        const int f = k < 2 ? k : k + 2;
+        float v00 = __ldg(s00 + f), v10 = __ldg(s10 + f);
+        float v01 = __ldg(s01 + f), v11 = __ldg(s11 + f);
+        if (f == 0) {
+            v00 = __fmaf_rn(d_left, ratio, v00);
+            v10 = __fmaf_rn(d_right, ratio, v10);
+            v01 = __fmaf_rn(d_left, ratio, v01);
+            v11 = __fmaf_rn(d_right, ratio, v11);
+        } else if (f == 1) {
+            v00 = __fmaf_rn(d_top, ratio, v00);
+            v10 = __fmaf_rn(d_top, ratio, v10);
+            v01 = __fmaf_rn(d_bottom, ratio, v01);
+            v11 = __fmaf_rn(d_bottom, ratio, v11);
+        }
+        const float upper = __fmaf_rn(__fsub_rn(v10, v00), tx, v00);
+        const float lower = __fmaf_rn(__fsub_rn(v11, v01), tx, v01);
+        seg[k] = __fmaf_rn(__fsub_rn(lower, upper), ty, upper);
+    }
+    return RaySegment{seg[0], seg[1], seg[2],  seg[3],  seg[4],  seg[5],  seg[6],  seg[7],
+                      seg[8], seg[9], seg[10], seg[11], seg[12], seg[13], seg[14], seg[15]};
+}
+
+// hierarchy_maximum (cuda_backend.py:656-874): the maximum slope along one
+// ray over one DEM, starting from `current` (-1e30 for none).  Table gives
+// side(l), fallback(l), out_step(l) and cells(l).
+template <bool kCount, bool kLadder, class Table>
+__device__ __forceinline__ float march_dem(const Table &table, const DemView &dem,
+                                           const RaySegment &g, int pass_index,
+                                           float observer_z, float current, unsigned &visits,
+                                           unsigned &samples, unsigned &steps) {
+    const float radius = dem.radius;
+    const float resolution = dem.resolution;
+    const float observer_radius = __fadd_rn(radius, observer_z);
+    const float inverse_denominator = __frcp_rn(__fmul_rn(2.0f, observer_radius));
+    const float *__restrict__ cells = dem.cells;
+    float s = g.s_start > 0.001f ? g.s_start : 0.001f;
+    const float minimum_step = __fmul_rn(__fmul_rn(0.5f, resolution), 0.001f);
+    const float primary_far_step = __fmul_rn(__fmul_rn(0.8f, resolution), 0.001f);
+    const float last_x = static_cast<float>(dem.width - 1);
+    const float last_y = static_cast<float>(dem.height - 1);
+    const int top_level = dem.level_count - 1;
+    int level_hint = top_level;
+    while (s <= g.s_end) {
+        if (kCount) ++steps;
+        const float delta = __fsub_rn(s, g.s_start);
+        const float px = quartic(g.start_x, g.a1, g.a2, g.a3, g.a4, delta);
+        const float py = quartic(g.start_y, g.b1, g.b2, g.b3, g.b4, delta);
+        // NaN fails every comparison, as the reference's isnan tests do.
+        if (!(px >= 0.0f && py >= 0.0f && px < last_x && py < last_y)) break;
+        const float planar_x = __fmul_rn(__fsub_rn(px, g.start_x), resolution);
+        const float planar_y = __fmul_rn(__fsub_rn(py, g.start_y), resolution);
+        const float planar_m = hypot_fused(planar_x, planar_y);
+        const bool near = s < 0.5f;
+        float true_m;
+        if (near) {
+            true_m = __fmul_rn(s, 1000.0f);
+        } else {
+            const float pm2 = __fmul_rn(planar_m, planar_m);
+            const float pm3 = __fmul_rn(pm2, planar_m);
+            float chord = __fmaf_rn(g.c1, planar_m, __fmul_rn(g.c2, pm2));
+            chord = __fmaf_rn(g.c3, pm3, chord);
+            true_m = __fmaf_rn(g.s_start_chord, 1000.0f, chord);
+        }
+        const float footprint = __fmul_rn(true_m, 0.004363323129985824f);
+        // The reference scans down from the top level to the largest level
+        // whose side fits the footprint (or 0).  Sides grow with the level,
+        // so that level is also found by moving up or down from the previous
+        // step's level, which usually takes one comparison.
+        int level = level_hint;
+        while (level < top_level && table.side(level + 1) <= footprint) ++level;
+        while (level > 0 && !(table.side(level) <= footprint)) --level;
+        level_hint = level;
+        // The tangent and its reciprocals depend only on delta.
+        const float dx = quartic_tangent(g.a1, g.a2, g.a3, g.a4, delta);
+        const float dy = quartic_tangent(g.b1, g.b2, g.b3, g.b4, delta);
+        const float inv_x = fabsf(dx) > 1e-8f ? __frcp_rn(dx) : 1e30f;
+        const float inv_y = fabsf(dy) > 1e-8f ? __frcp_rn(dy) : 1e30f;
+        const int ipx = static_cast<int>(px), ipy = static_cast<int>(py);
+        bool ray_out = false;
+        for (;;) {
+            const int4 L = table.cells(level);
+            const int shift = level * 2;
+            const int cx = ipx >> shift, cy = ipy >> shift;
+            if (kCount) ++visits;
+            if (cx >= L.y || cy >= L.z) {  // cx, cy >= 0 since px, py >= 0
+                s = __fadd_rn(s, table.out_step(level));
+                ray_out = true;
+                break;
+            }
+            const float maximum_height = four_cell_bound(cells, L, cx, cy);
+            const float skip =
+                cell_exit_advance(shift, cx, cy, px, py, inv_x, inv_y, table.fallback(level));
+            bool culled = maximum_height < -20000.0f;
+            if (!culled) {
+                const float scale_f = static_cast<float>(1 << shift);
+                float true_near = __fmaf_rn(-scale_f, resolution, true_m);
+                true_near = true_near > 1.0f ? true_near : 1.0f;
+                culled = bound_culled(near, true_near, maximum_height, radius, observer_z,
+                                      observer_radius, inverse_denominator, current);
+            }
+            if (culled) {
+                float advance = skip;
+                if (kLadder) {
+                    advance = ladder_advance<kCount>(table, cells, level, top_level, ipx, ipy,
+                                                     px, py, inv_x, inv_y, near, true_m, radius,
+                                                     observer_z, observer_radius, current, skip,
+                                                     visits);
+                }
+                s = __fadd_rn(s, advance);
+                break;
+            }
+            if (level == 0) {
+                if (kCount) ++samples;
+                const float height = bilinear(cells, dem.width, dem.height, px, py);
+                float slope = -1e30f;
+                if (height > -20000.0f) {
+                    slope = near ? __fdiv_rn(__fsub_rn(height, observer_z), true_m)
+                                 : sample_slope(true_m, height, radius, observer_radius);
+                    if (slope > current) current = slope;
+                }
+                const float magnitude = hypot_fused(dx, dy);
+                const float pixel_step = magnitude > 1e-6f ? __frcp_rn(magnitude) : 0.0005f;
+                const float margin = __fsub_rn(current, slope);
+                const float margin_step =
+                    margin > 0.0f
+                        ? __fdiv_rn(__fmul_rn(__fmul_rn(margin, true_m), 1.732f), 1000.0f)
+                        : 0.0f;
+                const float angular_step = __fdiv_rn(__fmul_rn(true_m, 0.00151f), 1000.0f);
+                const float inner = margin_step < angular_step ? margin_step : angular_step;
+                float advance = pixel_step > inner ? pixel_step : inner;
+                if (near) advance = __fmul_rn(advance, 0.25f);
+                const float floor_step =
+                    (pass_index == 0 && true_m >= 100.0f) ? primary_far_step : minimum_step;
+                advance = advance > floor_step ? advance : floor_step;
+                s = __fadd_rn(s, advance);
+                break;
+            }
+            --level;
+        }
+        if (ray_out) break;
+    }
+    return current;
+}
+
+}  // namespace ls200

@@ -24,13 +24,36 @@ from ._native import CudaBackendError, CudaExecutionError, call, library
 from .contract import PyramidArrays, map_parameters, projection_parameters
 
 __all__ = ["CudaBackendError", "CudaExecutionError", "CudaDeviceInfo", "CudaSession",
-           "DeviceDem"]
+           "DeviceDem", "SiteTile", "TRAVERSALS"]
+
+#: Traversals of the batched march: the reference's, and the skip ladder.
+TRAVERSALS = {"exact": 0, "ladder": 1}
 
 
 @dataclass(frozen=True, slots=True)
 class CudaDeviceInfo:
     name: str
     compute_capability: tuple[int, int]
+
+
+@dataclass(frozen=True, slots=True)
+class SiteTile:
+    """One 128x128 tile of one site for :meth:`CudaSession.march_sites`."""
+
+    dems: tuple  # DeviceDem, pass order, primary first
+    tile_column: int
+    tile_row: int
+    maximum_distance_m: float = 1_000_000.0
+    observer_elevation_m: float = 0.0
+
+
+class _SiteTileStruct(ctypes.Structure):
+    """ls200_site_tile (include/ls200.h)."""
+
+    _fields_ = [("dems", ctypes.c_void_p), ("dem_count", ctypes.c_int),
+                ("tile_column", ctypes.c_int), ("tile_row", ctypes.c_int),
+                ("maximum_distance_m", ctypes.c_double),
+                ("observer_elevation_m", ctypes.c_float)]
 
 
 class DeviceDem:
@@ -311,6 +334,35 @@ class CudaSession:
         call("ls200_segments_device", self._ctx, handles, len(dems), int(tile_column),
              int(tile_row), int(tile_width), int(azimuth_count), float(maximum_distance_m),
              float(observer_elevation_m), int(subpatch_size), ctypes.c_void_p(device_segments))
+
+    def march_sites(self, tiles, *, device_out: int, azimuth_count: int = 1440,
+                    subpatch_size: int = 8, traversal: str = "ladder",
+                    degrees: bool = False) -> tuple[float, float]:
+        """Every tile of a multi-site batch in one persistent launch into
+        ``device_out`` (tile_count x 16384 x azimuth_count float32, pixel-major
+        per tile).  Returns (segment + setup seconds, march seconds)."""
+        if traversal not in TRAVERSALS:
+            raise ValueError(f"traversal must be one of {sorted(TRAVERSALS)}")
+        tiles = list(tiles)
+        if not tiles:
+            raise ValueError("at least one tile is required")
+        handle_arrays = []
+        structs = (_SiteTileStruct * len(tiles))()
+        for slot, tile in zip(structs, tiles):
+            handles = (ctypes.c_void_p * len(tile.dems))(*[d.handle.value for d in tile.dems])
+            handle_arrays.append(handles)
+            slot.dems = ctypes.cast(handles, ctypes.c_void_p)
+            slot.dem_count = len(tile.dems)
+            slot.tile_column = int(tile.tile_column)
+            slot.tile_row = int(tile.tile_row)
+            slot.maximum_distance_m = float(tile.maximum_distance_m)
+            slot.observer_elevation_m = float(tile.observer_elevation_m)
+        seconds = np.zeros(2, dtype=np.float64)
+        call("ls200_march_sites", self._ctx, ctypes.cast(structs, ctypes.c_void_p), len(tiles),
+             int(azimuth_count),
+             int(subpatch_size), TRAVERSALS[traversal], 1 if degrees else 0,
+             ctypes.c_void_p(device_out), seconds.ctypes.data)
+        return float(seconds[0]), float(seconds[1])
 
     def fp32_probe(self, iterations: int = 4096) -> float:
         """Measured FP32 FMA throughput of this device in TFLOP/s."""

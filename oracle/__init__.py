@@ -60,6 +60,17 @@ CF_LXS_ALT = 1 << 18
 CF_SHIFT = 1 << 19
 #: Superseded level-0 cell-exit step cap (only to pin the older golden capture).
 OPT_EXIT_CAP = 1 << 16
+#: Skip ladder of the batched traversal (no reference counterpart): a cull
+#: climbs to the largest culled ancestor cell before skipping.
+OPT_LADDER = 1 << 20
+
+
+def ladder_mask(cap: int = 0, min_km: int = 0, base: int | None = None) -> int:
+    """Production arithmetic with the skip ladder; ``cap`` limits the climb
+    (0 = up to the top level), ``min_km`` is the distance from which it acts."""
+    if not 0 <= cap <= 15 or not 0 <= min_km <= 15:
+        raise ValueError("ladder cap and distance must be between 0 and 15")
+    return (PRODUCTION_MASK if base is None else base) | OPT_LADDER | (cap << 24) | (min_km << 28)
 
 #: Contraction mask whose FP32 arithmetic reproduces the reference's golden
 #: production captures (tests/test_oracle_pins.py checks it).

@@ -49,7 +49,15 @@ enum {
     ORA_CF_LXS_ALT = 1u << 18, /* local_x^2: fuse dist*dist instead of z*z */
     ORA_CF_SHIFT = 1u << 19,   /* subpatch shift product into the shift add */
     ORA_OPT_EXIT_CAP = 1u << 16, /* superseded level-0 cell-exit step cap */
+    /* Skip ladder (this project's batched traversal, not the reference's):
+     * after a cull at level l, climb to the parent levels while their
+     * four-cell bound is culled too, and skip to the exit of the largest
+     * culled cell.  Bits 24..27 cap the climb (0 = up to the top level). */
+    ORA_OPT_LADDER = 1u << 20,
 };
+#define ORA_LADDER_CAP(mask) (((mask) >> 24) & 15u)
+/* Bits 28..31: the ladder acts only from this distance on, in km. */
+#define ORA_LADDER_MIN_M(mask) (1000.0 * (double)(((mask) >> 28) & 15u))
 
 typedef struct {
     const float *level0;

@@ -337,6 +337,176 @@ def lighting_benchmark(session, dems, segments, tiles, primary, args, world, ran
     return result
 
 
+SITES = 64
+SITE_TILES_PER_BATCH = 16
+SITE_BATCHES = 3  # one warm-up batch, then timed batches
+TUNE_TILES = 4
+ACCURACY_RAYS_PER_TILE = 512
+
+
+def multisite_benchmark(session, stream, args, world, rank):
+    """The uneven multi-site workload (64 sites, sides 256-2048 px at 5-40 m,
+    latitudes -83 to -89.5, one polar 240 m regional DEM, 200 km rays): each
+    batch is one tile from each of 16 sites.  Plain = per-tile device segments
+    + per-pass launches + transpose; batched = one persistent work-stealing
+    launch over the whole batch (reference traversal, then skip ladder), its
+    launch configuration chosen by the autotuner on part of the warm-up
+    batch.  All produce degrees in HBM and are timed with CUDA events."""
+    import torch
+    import torch.distributed as dist
+
+    from lunarscout_b200 import synthetic
+    from lunarscout_b200.autotune import tune_batch
+    from lunarscout_b200.cuda_backend import SiteTile
+
+    started = time.perf_counter()
+    specs = synthetic.multisite_specs(SITES)
+    grids = [synthetic.synthetic_dem(spec) for spec in specs]
+    regional = synthetic.polar_regional_dem()
+    log(f"[bench] {SITES} site DEMs in {time.perf_counter() - started:.1f}s")
+    regional_dev = session.upload_dem_grid(regional)
+    site_devs = [session.upload_dem_grid(grid) for grid in grids]
+    rng = np.random.default_rng(77 + rank)
+    batches, picks = [], []
+    for b in range(SITE_BATCHES):
+        tiles, chosen = [], []
+        for j in range(SITE_TILES_PER_BATCH):
+            site = (rank * SITE_TILES_PER_BATCH * SITE_BATCHES + b * SITE_TILES_PER_BATCH + j) % SITES
+            grid = grids[site]
+            tx = int(rng.integers(0, (grid.width + TILE - 1) // TILE)) * TILE
+            ty = int(rng.integers(0, (grid.height + TILE - 1) // TILE)) * TILE
+            tiles.append(SiteTile((site_devs[site], regional_dev), tx, ty, RANGE_M, OBSERVER_M))
+            chosen.append(site)
+        batches.append(tiles)
+        picks.append(chosen)
+    timed_rays = sum(min(TILE, grids[s].width - t.tile_column)
+                     * min(TILE, grids[s].height - t.tile_row) * AZIMUTHS
+                     for tiles, chosen in zip(batches[1:], picks[1:])
+                     for t, s in zip(tiles, chosen))
+    centers = (TILE // 8 + 2) ** 2
+    segments = torch.empty(AZIMUTHS * centers * 2 * 18, dtype=torch.float32, device="cuda")
+    out = torch.empty((SITE_TILES_PER_BATCH, TILE * TILE, AZIMUTHS), dtype=torch.float32,
+                      device="cuda")
+    torch.cuda.synchronize()
+
+    def plain(tiles):
+        for i, tile in enumerate(tiles):
+            dems = list(tile.dems)
+            session.generate_segments_device(dems, segments.data_ptr(),
+                                             tile_column=tile.tile_column,
+                                             tile_row=tile.tile_row, azimuth_count=AZIMUTHS,
+                                             maximum_distance_m=RANGE_M,
+                                             observer_elevation_m=OBSERVER_M)
+            session.march_all_passes_device(segments.data_ptr(), AZIMUTHS, centers, dems,
+                                            tile_column=tile.tile_column,
+                                            tile_row=tile.tile_row,
+                                            observer_elevation_m=OBSERVER_M,
+                                            device_out=out[i].data_ptr(), degrees=True)
+
+    def batched(traversal):
+        def run(tiles):
+            session.march_sites(tiles, device_out=out.data_ptr(), azimuth_count=AZIMUTHS,
+                                traversal=traversal, degrees=True)
+        return run
+
+    def timed(run):
+        run(batches[0])
+        torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
+        start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        start.record(stream)
+        for tiles in batches[1:]:
+            run(tiles)
+        end.record(stream)
+        torch.cuda.synchronize()
+        elapsed = start.elapsed_time(end) / 1000.0
+        if world > 1:
+            t = torch.tensor([elapsed], device="cuda", dtype=torch.float64)
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+            elapsed = float(t.item())
+        return world * timed_rays / elapsed, elapsed
+
+    tuned = tune_batch(session, batches[0][:TUNE_TILES], device_out=out.data_ptr(),
+                       azimuth_count=AZIMUTHS, traversal="ladder")
+    plain_value, plain_s = timed(plain)
+    exact_value, exact_s = timed(batched("exact"))
+    ladder_value, ladder_s = timed(batched("ladder"))
+    result = {
+        "metric": "multi-site horizon rays/s (uneven batch, 2 DEM passes, 200 km)",
+        "unit": "rays/s",
+        "plain_per_tile": plain_value,
+        "batched_exact": exact_value,
+        "batched_ladder": ladder_value,
+        "speedup_batched_vs_plain": ladder_value / plain_value,
+        "speedup_exact_vs_plain": exact_value / plain_value,
+        "seconds": {"plain": plain_s, "exact": exact_s, "ladder": ladder_s},
+        "launch_config": {"kernel": tuned.best.kernel, "refill": tuned.best.refill,
+                          "rays_per_job": tuned.best.rays_per_job,
+                          "min_blocks": tuned.best.min_blocks,
+                          "tuned_on": f"{TUNE_TILES} tiles of the warm-up batch, ladder",
+                          "candidates_ms": {
+                              f"{c.kernel}/{c.refill}/{c.rays_per_job}/{c.min_blocks}":
+                                  1000.0 * s for c, s in tuned.seconds.items()}},
+        "sites": SITES, "tiles_per_batch": SITE_TILES_PER_BATCH,
+        "timed_batches": SITE_BATCHES - 1, "rays_timed_per_rank": timed_rays,
+        "rays": "rays of pixels inside each site DEM (partial edge tiles count their valid part)",
+    }
+    if rank == 0 and world == 1 and not args.skip_cpu:
+        result["error_vs_fp64_deg"] = multisite_accuracy(session, grids, regional, batches[1],
+                                                         picks[1], out, batched)
+    for dem in site_devs + [regional_dev]:
+        dem.close()
+    return result
+
+
+def multisite_accuracy(session, grids, regional, tiles, chosen, out, batched):
+    """Horizon error of both traversals against the FP64 restatement of the
+    reference march on a bounded ray sample of the first timed batch."""
+    import oracle
+    from lunarscout_b200.contract import PyramidArrays, map_parameters, projection_parameters
+
+    def pyramid(dem):
+        mips, levels = oracle.build_pyramid(dem.elevation_m)
+        return PyramidArrays(dem.elevation_m, mips, levels, map_parameters(dem),
+                             projection_parameters(dem))
+
+    regional_pyramid = pyramid(regional)
+    values = {}
+    for traversal in ("exact", "ladder"):
+        batched(traversal)(tiles)
+        values[traversal] = out[:4].cpu().numpy()
+    rng = np.random.default_rng(9)
+    errors = {"exact": [], "ladder": []}
+    for i, (tile, site) in enumerate(list(zip(tiles, chosen))[:4]):
+        grid = grids[site]
+        width = min(TILE, grid.width - tile.tile_column)
+        height = min(TILE, grid.height - tile.tile_row)
+        rows = rng.integers(0, height, ACCURACY_RAYS_PER_TILE)
+        cols = rng.integers(0, width, ACCURACY_RAYS_PER_TILE)
+        pixels = (rows * TILE + cols).astype(np.int32)
+        azimuths = rng.integers(0, AZIMUTHS, ACCURACY_RAYS_PER_TILE).astype(np.int32)
+        segments = session.generate_segments(list(tile.dems), tile_column=tile.tile_column,
+                                             tile_row=tile.tile_row, azimuth_count=AZIMUTHS,
+                                             maximum_distance_m=RANGE_M,
+                                             observer_elevation_m=OBSERVER_M)
+        fp64, _ = oracle.march_all_passes(segments, [pyramid(grid), regional_pyramid],
+                                          tile_column=tile.tile_column, tile_row=tile.tile_row,
+                                          observer_elevation_m=OBSERVER_M, pixels=pixels,
+                                          azimuths=azimuths, precision="f64")
+        reference = np.degrees(np.arctan(fp64))
+        for traversal in errors:
+            got = values[traversal][i][pixels, azimuths].astype(np.float64)
+            finite = np.isfinite(reference) & np.isfinite(got)
+            errors[traversal].append(np.abs(got[finite] - reference[finite]))
+    summary = {}
+    for traversal, parts in errors.items():
+        e = np.concatenate(parts)
+        summary[traversal] = {"p99.9": float(np.quantile(e, 0.999)), "max": float(e.max()),
+                              "mean": float(e.mean()), "rays": int(e.size)}
+    return summary
+
+
 def run_ours(args):
     import torch
     import torch.distributed as dist
@@ -463,6 +633,9 @@ def run_ours(args):
     e2e_session.close()
 
     lighting = lighting_benchmark(session, dems, segments, tiles, primary, args, world, rank)
+    del segments
+    multisite = None if args.skip_multisite else multisite_benchmark(session, stream, args,
+                                                                     world, rank)
 
     fp32_peak = session.fp32_probe()
     pass_times = np.array(pass_times)
@@ -510,6 +683,7 @@ def run_ours(args):
             "clocks": clocks,
             "segment_generation_ms_per_tile": segment_seconds * 1000.0,
             "lightmap": lighting,
+            "multisite": multisite,
         }
         print(json.dumps(line), flush=True)
     session.close()
@@ -574,6 +748,34 @@ def run_profile_case():
     log("[bench] profile case done")
 
 
+def run_profile_multisite():
+    """Four tiles of the multi-site batch through the persistent march, exact
+    traversal then skip ladder (launches 2 and 4 are the marches); used under
+    ncu, never timed."""
+    import torch
+
+    from lunarscout_b200 import synthetic
+    from lunarscout_b200.cuda_backend import CudaSession, SiteTile
+
+    specs = synthetic.multisite_specs(SITES)[:4]
+    grids = [synthetic.synthetic_dem(spec) for spec in specs]
+    regional = synthetic.polar_regional_dem()
+    session = CudaSession(0)
+    regional_dev = session.upload_dem_grid(regional)
+    tiles = []
+    for grid in grids:
+        dev = session.upload_dem_grid(grid)
+        tiles.append(SiteTile((dev, regional_dev), (grid.width // 2 // TILE) * TILE,
+                              (grid.height // 2 // TILE) * TILE, RANGE_M, OBSERVER_M))
+    out = torch.empty(len(tiles) * RAYS_PER_TILE, dtype=torch.float32, device="cuda")
+    torch.cuda.synchronize()
+    for traversal in ("exact", "ladder"):
+        session.march_sites(tiles, device_out=out.data_ptr(), azimuth_count=AZIMUTHS,
+                            traversal=traversal, degrees=True)
+    session.close()
+    log("[bench] multisite profile case done")
+
+
 def main():
     parser = argparse.ArgumentParser()
     parser.add_argument("--gpus", type=int, default=1)
@@ -583,12 +785,18 @@ def main():
     parser.add_argument("--cpu-seconds", type=float, default=12.0)
     parser.add_argument("--reference-seconds", type=float, default=8.0)
     parser.add_argument("--skip-cpu", action="store_true")
-    parser.add_argument("--profile", action="store_true",
-                        help="small profiling case: one tile, two march steps, no timing")
+    parser.add_argument("--skip-multisite", action="store_true",
+                        help="leave out the uneven multi-site batched-vs-plain leg")
+    parser.add_argument("--profile", nargs="?", const="site", choices=("site", "multisite"),
+                        help="small profiling case, no timing: 'site' = one site-scale tile "
+                             "(two march steps, two lighting launches); 'multisite' = four "
+                             "tiles through the persistent march (exact, then ladder)")
     args = parser.parse_args()
     if args.warmup < 3:
         args.warmup = 3
-    if args.profile:
+    if args.profile == "multisite":
+        run_profile_multisite()
+    elif args.profile:
         run_profile_case()
     elif args.impl == "reference":
         run_reference(args)

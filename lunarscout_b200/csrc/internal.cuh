@@ -127,6 +127,11 @@ struct ls200_context {
     std::set<ls200_dem *> dems;  // live DEMs, released with the context
     ls200::LightingState *lighting = nullptr;
     ls200::CodecBuffers *codec = nullptr;
+    // Launch configuration of the persistent multi-site march.
+    int batch_kernel = 1;          // 0: one ray per lane, 1: dynamic ray fetching
+    int batch_refill = 8;          // lanes that must wait before a refill
+    int batch_rays_per_job = 128;  // rays a warp takes from the global counter
+    int batch_min_blocks = 8;      // resident 128-thread blocks per SM (8 or 6)
 };
 
 namespace ls200 {

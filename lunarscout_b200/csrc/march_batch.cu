@@ -55,6 +55,9 @@ struct SitesParams {
     long long jobs_per_tile, job_count;
     unsigned long long *next_job;
     unsigned long long *counters;
+    // ray-refill kernel: flat ray space, rays per job, refill threshold
+    long long total_rays, rays_per_job;
+    int refill_threshold;
 };
 
 // Level table read through the read-only path (each warp may be on a
@@ -124,6 +127,124 @@ __global__ void __launch_bounds__(128, 8) march_sites_kernel(const __grid_consta
         *out = value;
     }
     if (kCount) add_counters(P.counters, visits, samples, steps);
+}
+
+// The same march with dynamic ray fetching.  Rays of one warp finish at very
+// different times (with the skip ladder the longest of 32 adjacent rays does
+// about twice the mean work), so a lane whose ray (or DEM pass) ends does not
+// wait for the warp: once `refill_threshold` lanes wait, they take the next
+// rays of the warp's job (jobs of `rays_per_job` consecutive rays, taken from
+// the global counter) or begin their next pass, together, and every lane
+// then continues one march step at a time (march_step).  Per-ray arithmetic
+// is unchanged, so results equal the simple kernel's bit for bit.
+template <bool kCount, bool kLadder, int kMinBlocks>
+__global__ void __launch_bounds__(128, kMinBlocks)
+    march_sites_refill_kernel(const __grid_constant__ SitesParams P) {
+    const unsigned lane = threadIdx.x & 31;
+    const unsigned below = (1u << lane) - 1u;
+    const long long rays_per_tile = static_cast<long long>(kTilePixels) * P.azimuth_count;
+    long long pool_next = 0, pool_end = 0;  // warp-uniform
+    bool exhausted = false;                 // warp-uniform
+    enum { kIdle = 0, kBegin = 1, kMarch = 2 };
+    int phase = kIdle;
+    int t = 0, pixel = 0, azimuth = 0, d = 0, dem_count = 0;
+    float observer_z = 0.0f;
+    RaySegment g{};
+    DemView view{};
+    const LevelTable *table = nullptr;
+    MarchState st{0.0f, -1e30f, 0};
+    unsigned visits = 0, samples = 0, steps = 0;
+    for (;;) {
+        const unsigned waiting = __ballot_sync(0xffffffffu, phase != kMarch);
+        if (waiting == 0xffffffffu || __popc(waiting) >= P.refill_threshold) {
+            const unsigned idle = __ballot_sync(0xffffffffu, phase == kIdle);
+            if (idle != 0u) {
+                if (pool_next >= pool_end && !exhausted) {
+                    unsigned long long taken = 0;
+                    if (lane == 0) taken = atomicAdd(P.next_job, 1ull);
+                    const long long job =
+                        static_cast<long long>(__shfl_sync(0xffffffffu, taken, 0));
+                    const long long first = job * P.rays_per_job;
+                    if (first >= P.total_rays) {
+                        exhausted = true;
+                    } else {
+                        pool_next = first;
+                        pool_end = min(first + P.rays_per_job, P.total_rays);
+                    }
+                }
+                if (phase == kIdle) {
+                    const long long ray = pool_next + __popc(idle & below);
+                    if (ray < pool_end) {
+                        t = static_cast<int>(ray / rays_per_tile);
+                        const int r = static_cast<int>(ray - t * rays_per_tile);
+                        pixel = r % kTilePixels;
+                        azimuth = r / kTilePixels;
+                        const BatchTile &tile = P.tiles[t];
+                        const DemView &primary = P.dems[tile.dems[0]].view;
+                        const int row = pixel / kTileSide, column = pixel % kTileSide;
+                        if (tile.tile_column + column >= primary.width ||
+                            tile.tile_row + row >= primary.height) {
+                            // Outside the primary DEM: the -inf sentinel.
+                            tile.out[static_cast<size_t>(pixel) * P.azimuth_count + azimuth] =
+                                -INFINITY;
+                        } else {
+                            observer_z = __fadd_rn(
+                                bilinear(primary.cells, primary.width, primary.height,
+                                         static_cast<float>(tile.tile_column + column),
+                                         static_cast<float>(tile.tile_row + row)),
+                                tile.observer_elevation);
+                            d = 0;
+                            dem_count = tile.dem_count;
+                            st.current = -1e30f;
+                            phase = kBegin;
+                        }
+                    }
+                }
+                pool_next = min(pool_end, pool_next + __popc(idle));
+            }
+            if (phase == kBegin) {
+                const BatchTile &tile = P.tiles[t];
+                const DemView &primary = P.dems[tile.dems[0]].view;
+                const BatchDem &dem = P.dems[tile.dems[d]];
+                view = dem.view;
+                table = &dem.table;
+                const float ratio = __fdiv_rn(primary.column_res, view.column_res);
+                g = interpolate_segment(tile.segments, P.center_count, tile.dem_count, d,
+                                        azimuth, pixel % kTileSide, pixel / kTileSide,
+                                        tile.tile_column, tile.tile_row, kTileSide, P.subpatch,
+                                        primary.width, primary.height, ratio);
+                st = begin_pass(view, g, st.current);
+                phase = kMarch;
+            }
+            if (__ballot_sync(0xffffffffu, phase != kIdle) == 0u && exhausted &&
+                pool_next >= pool_end)
+                break;
+        }
+        if (phase == kMarch) {
+            if (!march_step<kCount, kLadder>(GlobalLevels{table}, view, g, d, observer_z, st,
+                                             visits, samples, steps)) {
+                if (++d < dem_count) {
+                    phase = kBegin;
+                } else {
+                    float value = st.current > -1e29f ? st.current : -INFINITY;
+                    if (P.degrees && !isinf(value)) value = __fmul_rn(atanf(value), kSlopeDegrees);
+                    P.tiles[t].out[static_cast<size_t>(pixel) * P.azimuth_count + azimuth] = value;
+                    phase = kIdle;
+                }
+            }
+        }
+    }
+    if (kCount) add_counters(P.counters, visits, samples, steps);
+}
+
+template <bool kCount, bool kLadder, int kMinBlocks>
+static void launch_refill(ls200_context *ctx, const SitesParams &P) {
+    int per_sm = 0;
+    LS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+        &per_sm, march_sites_refill_kernel<kCount, kLadder, kMinBlocks>, 128, 0));
+    const int blocks = ctx->props.multiProcessorCount * (per_sm > 0 ? per_sm : 1);
+    march_sites_refill_kernel<kCount, kLadder, kMinBlocks><<<blocks, 128, 0, ctx->stream>>>(P);
+    LS_CUDA(cudaGetLastError());
 }
 
 template <bool kCount, bool kLadder>
@@ -261,13 +382,35 @@ extern "C" ls200_status ls200_march_sites(ls200_context *ctx, const ls200_site_t
         P.job_count = P.jobs_per_tile * tile_count;
         P.next_job = reinterpret_cast<unsigned long long *>(scratch + off_job);
         P.counters = ctx->counters.as<unsigned long long>();
+        P.total_rays = static_cast<long long>(kTilePixels) * azimuth_count * tile_count;
+        P.rays_per_job = ctx->batch_rays_per_job;
+        P.refill_threshold = ctx->batch_refill;
         reset_counters(ctx);
-        if (ctx->counting) {
-            if (traversal) launch_sites<true, true>(ctx, P);
-            else launch_sites<true, false>(ctx, P);
+        const bool ladder = traversal != 0;
+        if (ctx->batch_kernel == 0) {
+            if (ctx->counting) {
+                if (ladder) launch_sites<true, true>(ctx, P);
+                else launch_sites<true, false>(ctx, P);
+            } else {
+                if (ladder) launch_sites<false, true>(ctx, P);
+                else launch_sites<false, false>(ctx, P);
+            }
+        } else if (ctx->batch_min_blocks == 6) {
+            if (ctx->counting) {
+                if (ladder) launch_refill<true, true, 6>(ctx, P);
+                else launch_refill<true, false, 6>(ctx, P);
+            } else {
+                if (ladder) launch_refill<false, true, 6>(ctx, P);
+                else launch_refill<false, false, 6>(ctx, P);
+            }
         } else {
-            if (traversal) launch_sites<false, true>(ctx, P);
-            else launch_sites<false, false>(ctx, P);
+            if (ctx->counting) {
+                if (ladder) launch_refill<true, true, 8>(ctx, P);
+                else launch_refill<true, false, 8>(ctx, P);
+            } else {
+                if (ladder) launch_refill<false, true, 8>(ctx, P);
+                else launch_refill<false, false, 8>(ctx, P);
+            }
         }
         if (seconds) LS_CUDA(cudaEventRecord(ctx->events[2], ctx->stream));
         // The host tables above must outlive their copies.
@@ -280,5 +423,34 @@ extern "C" ls200_status ls200_march_sites(ls200_context *ctx, const ls200_site_t
             seconds[1] = ms / 1000.0;
         }
         resolve_counters(ctx);
+    });
+}
+
+extern "C" ls200_status ls200_set_batch_config(ls200_context *ctx, int kernel, int refill,
+                                               int rays_per_job, int min_blocks) {
+    return guard([&] {
+        LS_REQUIRE(ctx, "NULL argument");
+        LS_REQUIRE(kernel == 0 || kernel == 1, "kernel must be 0 or 1");
+        LS_REQUIRE(refill >= 1 && refill <= 32, "refill threshold must be between 1 and 32");
+        LS_REQUIRE(rays_per_job >= 32 && rays_per_job % 32 == 0 && rays_per_job <= (1 << 20),
+                   "rays_per_job must be a multiple of 32 up to 2^20");
+        LS_REQUIRE(min_blocks == 6 || min_blocks == 8, "min_blocks must be 6 or 8");
+        std::lock_guard<std::mutex> hold(ctx->lock);
+        ctx->batch_kernel = kernel;
+        ctx->batch_refill = refill;
+        ctx->batch_rays_per_job = rays_per_job;
+        ctx->batch_min_blocks = min_blocks;
+    });
+}
+
+extern "C" ls200_status ls200_get_batch_config(ls200_context *ctx, int *kernel, int *refill,
+                                               int *rays_per_job, int *min_blocks) {
+    return guard([&] {
+        LS_REQUIRE(ctx && kernel && refill && rays_per_job && min_blocks, "NULL argument");
+        std::lock_guard<std::mutex> hold(ctx->lock);
+        *kernel = ctx->batch_kernel;
+        *refill = ctx->batch_refill;
+        *rays_per_job = ctx->batch_rays_per_job;
+        *min_blocks = ctx->batch_min_blocks;
     });
 }

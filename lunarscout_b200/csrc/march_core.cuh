@@ -366,33 +366,48 @@ __device__ __forceinline__ RaySegment interpolate_segment(
                       seg[8], seg[9], seg[10], seg[11], seg[12], seg[13], seg[14], seg[15]};
 }
 
-// hierarchy_maximum (cuda_backend.py:656-874): the maximum slope along one
-// ray over one DEM, starting from `current` (-1e30 for none).  Table gives
-// side(l), fallback(l), out_step(l) and cells(l).
+// The state of one ray within one DEM pass of hierarchy_maximum.
+struct MarchState {
+    float s;            // path position (km)
+    float current;      // maximum slope so far (-1e30 for none)
+    int level_hint;     // level of the previous step
+};
+
+__device__ __forceinline__ MarchState begin_pass(const DemView &dem, const RaySegment &g,
+                                                 float current) {
+    return MarchState{g.s_start > 0.001f ? g.s_start : 0.001f, current, dem.level_count - 1};
+}
+
+// One outer iteration of hierarchy_maximum (cuda_backend.py:672-867): one ray
+// position, the level descent (and with kLadder the climb) and the advance.
+// Returns false, leaving `st` untouched, when the pass is over (past s_end,
+// outside the DEM, or the cell left the level grid).
 template <bool kCount, bool kLadder, class Table>
-__device__ __forceinline__ float march_dem(const Table &table, const DemView &dem,
+__device__ __forceinline__ bool march_step(const Table &table, const DemView &dem,
                                            const RaySegment &g, int pass_index,
-                                           float observer_z, float current, unsigned &visits,
+                                           float observer_z, MarchState &st, unsigned &visits,
                                            unsigned &samples, unsigned &steps) {
     const float radius = dem.radius;
     const float resolution = dem.resolution;
     const float observer_radius = __fadd_rn(radius, observer_z);
     const float inverse_denominator = __frcp_rn(__fmul_rn(2.0f, observer_radius));
     const float *__restrict__ cells = dem.cells;
-    float s = g.s_start > 0.001f ? g.s_start : 0.001f;
     const float minimum_step = __fmul_rn(__fmul_rn(0.5f, resolution), 0.001f);
     const float primary_far_step = __fmul_rn(__fmul_rn(0.8f, resolution), 0.001f);
     const float last_x = static_cast<float>(dem.width - 1);
     const float last_y = static_cast<float>(dem.height - 1);
     const int top_level = dem.level_count - 1;
-    int level_hint = top_level;
-    while (s <= g.s_end) {
+    float s = st.s;
+    float current = st.current;
+    int level_hint = st.level_hint;
+    if (!(s <= g.s_end)) return false;
+    {
         if (kCount) ++steps;
         const float delta = __fsub_rn(s, g.s_start);
         const float px = quartic(g.start_x, g.a1, g.a2, g.a3, g.a4, delta);
         const float py = quartic(g.start_y, g.b1, g.b2, g.b3, g.b4, delta);
         // NaN fails every comparison, as the reference's isnan tests do.
-        if (!(px >= 0.0f && py >= 0.0f && px < last_x && py < last_y)) break;
+        if (!(px >= 0.0f && py >= 0.0f && px < last_x && py < last_y)) return false;
         const float planar_x = __fmul_rn(__fsub_rn(px, g.start_x), resolution);
         const float planar_y = __fmul_rn(__fsub_rn(py, g.start_y), resolution);
         const float planar_m = hypot_fused(planar_x, planar_y);
@@ -483,9 +498,27 @@ __device__ __forceinline__ float march_dem(const Table &table, const DemView &de
             }
             --level;
         }
-        if (ray_out) break;
+        if (ray_out) return false;
     }
-    return current;
+    st.s = s;
+    st.current = current;
+    st.level_hint = level_hint;
+    return true;
+}
+
+// hierarchy_maximum (cuda_backend.py:656-874): the maximum slope along one
+// ray over one DEM, starting from `current` (-1e30 for none).  Table gives
+// side(l), fallback(l), out_step(l) and cells(l).
+template <bool kCount, bool kLadder, class Table>
+__device__ __forceinline__ float march_dem(const Table &table, const DemView &dem,
+                                           const RaySegment &g, int pass_index,
+                                           float observer_z, float current, unsigned &visits,
+                                           unsigned &samples, unsigned &steps) {
+    MarchState st = begin_pass(dem, g, current);
+    while (march_step<kCount, kLadder>(table, dem, g, pass_index, observer_z, st, visits,
+                                       samples, steps)) {
+    }
+    return st.current;
 }
 
 }  // namespace ls200

@@ -24,7 +24,7 @@ from ._native import CudaBackendError, CudaExecutionError, call, library
 from .contract import PyramidArrays, map_parameters, projection_parameters
 
 __all__ = ["CudaBackendError", "CudaExecutionError", "CudaDeviceInfo", "CudaSession",
-           "DeviceDem", "SiteTile", "TRAVERSALS"]
+           "DeviceDem", "SiteTile", "BatchConfig", "TRAVERSALS"]
 
 #: Traversals of the batched march: the reference's, and the skip ladder.
 TRAVERSALS = {"exact": 0, "ladder": 1}
@@ -45,6 +45,19 @@ class SiteTile:
     tile_row: int
     maximum_distance_m: float = 1_000_000.0
     observer_elevation_m: float = 0.0
+
+
+@dataclass(frozen=True, slots=True)
+class BatchConfig:
+    """Launch configuration of the persistent multi-site march: ``kernel`` 0
+    (one ray per lane) or 1 (dynamic ray fetching), the ``refill`` threshold
+    (waiting lanes of 32), ``rays_per_job`` taken per work-counter increment,
+    and ``min_blocks`` resident 128-thread blocks per SM (8 or 6)."""
+
+    kernel: int = 1
+    refill: int = 8
+    rays_per_job: int = 128
+    min_blocks: int = 8
 
 
 class _SiteTileStruct(ctypes.Structure):
@@ -363,6 +376,16 @@ class CudaSession:
              int(subpatch_size), TRAVERSALS[traversal], 1 if degrees else 0,
              ctypes.c_void_p(device_out), seconds.ctypes.data)
         return float(seconds[0]), float(seconds[1])
+
+    def set_batch_config(self, config: BatchConfig) -> None:
+        """Launch configuration of :meth:`march_sites` (results do not depend on it)."""
+        call("ls200_set_batch_config", self._ctx, int(config.kernel), int(config.refill),
+             int(config.rays_per_job), int(config.min_blocks))
+
+    def batch_config(self) -> BatchConfig:
+        values = [ctypes.c_int() for _ in range(4)]
+        call("ls200_get_batch_config", self._ctx, *[ctypes.byref(v) for v in values])
+        return BatchConfig(*(v.value for v in values))
 
     def fp32_probe(self, iterations: int = 4096) -> float:
         """Measured FP32 FMA throughput of this device in TFLOP/s."""

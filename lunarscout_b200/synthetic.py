@@ -144,6 +144,33 @@ def regional_dem(size: int = 2000, resolution_m: float = 240.0, *, seed: int = 2
                                           tilt_m=2000.0, seed=seed + 1000))
 
 
+def multisite_specs(count: int = 64, *, seed: int = 64) -> list[SyntheticDemSpec]:
+    """The uneven multi-site batch: sides log-uniform in [256, 2048] px,
+    resolution from {5, 10, 20, 40} m, latitudes -83 to -89.5 deg, any
+    longitude; crater sizes scale with the site extent."""
+    rng = np.random.default_rng(seed)
+    specs = []
+    for i in range(count):
+        size = int(round(math.exp(rng.uniform(math.log(256), math.log(2048)))))
+        resolution = float(rng.choice((5.0, 10.0, 20.0, 40.0)))
+        extent = size * resolution
+        specs.append(SyntheticDemSpec(
+            size, resolution, latitude_deg=float(rng.uniform(-89.5, -83.0)),
+            longitude_deg=float(rng.uniform(0.0, 360.0)),
+            craters=max(8, size * size // 20000), crater_max_m=min(8000.0, extent / 4.0),
+            seed=seed * 1000 + i))
+    return specs
+
+
+def polar_regional_dem(size: int = 2000, resolution_m: float = 240.0, *,
+                       seed: int = 2) -> DemGrid:
+    """Regional DEM centred on the pole (480 km across at the defaults), so
+    that it surrounds every site of the multi-site batch."""
+    return synthetic_dem(SyntheticDemSpec(size, resolution_m, latitude_deg=-90.0,
+                                          longitude_deg=0.0, sigma_m=1200.0, craters=0,
+                                          tilt_m=2000.0, seed=seed + 1000))
+
+
 def hours_between(start: str, stop: str, step_hours: float) -> np.ndarray:
     """Elapsed hours of a regular time axis [start, stop] (inclusive)."""
     t0 = np.datetime64(start)

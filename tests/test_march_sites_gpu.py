@@ -157,3 +157,43 @@ def test_batch_validation(batch, cuda_session):
                                  azimuth_count=AZ)
     with pytest.raises(ValueError):
         cuda_session.march_sites([], device_out=out.data_ptr(), azimuth_count=AZ)
+
+
+@pytest.mark.parametrize("traversal", ["exact", "ladder"])
+def test_results_are_invariant_across_launch_configurations(batch, cuda_session, traversal):
+    from lunarscout_b200.autotune import DEFAULT_CANDIDATES
+
+    tiles, _ = batch
+    default = cuda_session.batch_config()
+    reference = _run(cuda_session, tiles, traversal)
+    try:
+        for config in DEFAULT_CANDIDATES:
+            cuda_session.set_batch_config(config)
+            np.testing.assert_array_equal(_run(cuda_session, tiles, traversal), reference,
+                                          err_msg=str(config))
+    finally:
+        cuda_session.set_batch_config(default)
+
+
+def test_autotuner_times_every_candidate_and_applies_the_winner(batch, cuda_session):
+    import torch
+
+    from lunarscout_b200.autotune import DEFAULT_CANDIDATES, tune_batch
+    from lunarscout_b200.cuda_backend import BatchConfig
+
+    tiles, _ = batch
+    default = cuda_session.batch_config()
+    out = torch.empty(len(tiles) * 16384 * AZ, dtype=torch.float32, device="cuda")
+    torch.cuda.synchronize()
+    try:
+        result = tune_batch(cuda_session, tiles, device_out=out.data_ptr(), azimuth_count=AZ)
+        assert set(result.seconds) == set(DEFAULT_CANDIDATES)
+        assert all(s > 0.0 for s in result.seconds.values())
+        assert cuda_session.batch_config() == result.best
+    finally:
+        cuda_session.set_batch_config(default)
+    with pytest.raises(ValueError):
+        cuda_session.set_batch_config(BatchConfig(1, 8, 100, 8))
+    with pytest.raises(ValueError):
+        cuda_session.set_batch_config(BatchConfig(1, 8, 128, 7))
+    assert cuda_session.batch_config() == default

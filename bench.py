@@ -441,12 +441,11 @@ def multisite_benchmark(session, stream, args, world, rank):
         "speedup_batched_vs_plain": ladder_value / plain_value,
         "speedup_exact_vs_plain": exact_value / plain_value,
         "seconds": {"plain": plain_s, "exact": exact_s, "ladder": ladder_s},
-        "launch_config": {"kernel": tuned.best.kernel, "refill": tuned.best.refill,
-                          "rays_per_job": tuned.best.rays_per_job,
+        "launch_config": {"lanes_per_azimuth": tuned.best.lanes_per_azimuth,
                           "min_blocks": tuned.best.min_blocks,
                           "tuned_on": f"{TUNE_TILES} tiles of the warm-up batch, ladder",
                           "candidates_ms": {
-                              f"{c.kernel}/{c.refill}/{c.rays_per_job}/{c.min_blocks}":
+                              f"lanes{c.lanes_per_azimuth}/blocks{c.min_blocks}":
                                   1000.0 * s for c, s in tuned.seconds.items()}},
         "sites": SITES, "tiles_per_batch": SITE_TILES_PER_BATCH,
         "timed_batches": SITE_BATCHES - 1, "rays_timed_per_rank": timed_rays,

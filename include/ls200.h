@@ -165,16 +165,12 @@ ls200_status ls200_march_sites(ls200_context *ctx, const ls200_site_tile *tiles,
                                int degrees, void *device_out, double *seconds);
 
 /* Launch configuration of ls200_march_sites for this context (results do
- * not depend on it): kernel 0 = one ray per lane, 1 = dynamic ray fetching
- * (waiting lanes take new rays / begin their next pass together once
- * `refill` of the 32 lanes wait); `rays_per_job` rays per take from the
- * global work counter (multiple of 32); `min_blocks` resident 128-thread
- * blocks per SM, 8 (64 registers) or 6 (80 registers).  Chosen by the
- * autotuner; defaults 1, 8, 128, 8. */
-ls200_status ls200_set_batch_config(ls200_context *ctx, int kernel, int refill,
-                                    int rays_per_job, int min_blocks);
-ls200_status ls200_get_batch_config(ls200_context *ctx, int *kernel, int *refill,
-                                    int *rays_per_job, int *min_blocks);
+ * not depend on it): `lanes_per_azimuth` = how many adjacent pixels of one
+ * azimuth a 32-ray warp job holds (a power of two from 1 to 32; the job then
+ * spans 32 / lanes_per_azimuth azimuths), `min_blocks` = resident 128-thread blocks per SM, 8 (64
+ * registers) or 6 (80 registers).  Chosen by the autotuner; defaults 32, 8. */
+ls200_status ls200_set_batch_config(ls200_context *ctx, int lanes_per_azimuth, int min_blocks);
+ls200_status ls200_get_batch_config(ls200_context *ctx, int *lanes_per_azimuth, int *min_blocks);
 
 /* slope -> degrees, float32(atan(s) * float32(180/pi)), -inf preserved:
  * src/lunarscout/_numba_horizon/contract.py:362-371 (HorizonBuffers.degrees) */

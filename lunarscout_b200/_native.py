@@ -87,8 +87,8 @@ SIGNATURES: dict[str, list] = {
     "ls200_slopes_to_degrees": [_vp, _f32p, _i64, _f32p],
     "ls200_horizon_tile": [_vp, _vp, _i, _i, _i, _i, _d, _f, _i, _i, _vp, _i64, _vp],
     "ls200_march_sites": [_vp, _vp, _i, _i, _i, _i, _i, _vp, _vp],
-    "ls200_set_batch_config": [_vp, _i, _i, _i, _i],
-    "ls200_get_batch_config": [_vp, _vp, _vp, _vp, _vp],
+    "ls200_set_batch_config": [_vp, _i, _i],
+    "ls200_get_batch_config": [_vp, _vp, _vp],
     "ls200_cbin_encode": [_vp, _f32p, _vp, _i64, _vp],
     "ls200_cbin_encode_device": [_vp, _vp, _vp, _vp],
     "ls200_cbin_decode": [_vp, _vp, _i64, _f32p],

@@ -1,10 +1,9 @@
 """Autotuner of the persistent multi-site march's launch configuration.
 
 The batched march (``CudaSession.march_sites``) has launch parameters that
-change its speed but never its results: the kernel variant (one ray per lane,
-or dynamic ray fetching), the refill threshold (how many of a warp's 32 lanes
-must wait before they take new rays together), the rays a warp takes per
-work-counter increment, and the resident blocks per SM (8 blocks at 64
+change its speed but never its results: how the 32 rays of a warp job are
+laid out (L adjacent pixels x 32/L adjacent azimuths: the azimuths per
+warp) and the resident blocks per SM (8 blocks at 64
 registers, or 6 at 80).  ``tune_batch`` times each candidate on a sample
 batch with CUDA events (the march seconds the library reports) and keeps the
 fastest; results may be cached per device and workload key in a JSON file.
@@ -20,13 +19,9 @@ from pathlib import Path
 
 from .cuda_backend import BatchConfig
 
-#: The default search space: the one-ray-per-lane kernel, and the refill
-#: kernel over thresholds, job sizes and occupancies.
-DEFAULT_CANDIDATES: tuple[BatchConfig, ...] = (
-    (BatchConfig(0, 8, 128, 8),)
-    + tuple(BatchConfig(1, refill, rays, blocks)
-            for refill in (4, 8, 16) for rays in (128, 512) for blocks in (8, 6))
-)
+#: The default search space: lane layouts x occupancies, the default first.
+DEFAULT_CANDIDATES: tuple[BatchConfig, ...] = tuple(
+    BatchConfig(lanes, blocks) for lanes in (32, 16, 8, 4, 2, 1) for blocks in (8, 6))
 
 
 @dataclass(frozen=True, slots=True)

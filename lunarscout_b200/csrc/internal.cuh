@@ -128,10 +128,8 @@ struct ls200_context {
     ls200::LightingState *lighting = nullptr;
     ls200::CodecBuffers *codec = nullptr;
     // Launch configuration of the persistent multi-site march.
-    int batch_kernel = 1;          // 0: one ray per lane, 1: dynamic ray fetching
-    int batch_refill = 8;          // lanes that must wait before a refill
-    int batch_rays_per_job = 128;  // rays a warp takes from the global counter
-    int batch_min_blocks = 8;      // resident 128-thread blocks per SM (8 or 6)
+    int batch_lanes_per_azimuth = 32;  // pixels of one azimuth in a 32-ray job (1..32)
+    int batch_min_blocks = 8;          // resident 128-thread blocks per SM (8 or 6)
 };
 
 namespace ls200 {

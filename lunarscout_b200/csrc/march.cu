@@ -80,7 +80,7 @@ __global__ void __launch_bounds__(128, 8) march_pass_kernel(const __grid_constan
     const DemView dem{P.cells, P.width, P.height, P.level_count, resolution, column_res,
                       P.radius};
     unsigned visits = 0, samples = 0, steps = 0;
-    current = march_dem<kCount, false>(SharedLevels{table}, dem, g, P.pass_index, observer_z,
+    current = march_dem<kCount, kReference>(SharedLevels{table}, dem, g, P.pass_index, observer_z,
                                        current, visits, samples, steps);
     *out = current > -1e29f ? current : -INFINITY;
     if (kCount) add_counters(P.counters, visits, samples, steps);

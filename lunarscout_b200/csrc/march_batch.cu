@@ -14,6 +14,11 @@
 // the footprint-limited steps of long rays; its results are checked against
 // its own CPU restatement (oracle flag OPT_LADDER) and their distance from
 // the FP64 restatement is measured beside the reference traversal's.
+//
+// Launch configuration (autotuned, never changing results): how the 32 lanes
+// of a job map onto rays (L adjacent pixels x 32/L adjacent azimuths, L a
+// power of two up to 32), and the resident blocks per SM (8 at 64 registers,
+// 6 at 80).
 #include "march_core.cuh"
 
 #include <map>
@@ -52,12 +57,10 @@ struct SitesParams {
     const BatchDem *dems;
     const BatchTile *tiles;
     int azimuth_count, center_count, subpatch, degrees;
-    long long jobs_per_tile, job_count;
+    int lanes_per_azimuth;  // 1..32 (power of two): pixels of one azimuth in a job
+    long long pixel_groups, jobs_per_tile, job_count;
     unsigned long long *next_job;
     unsigned long long *counters;
-    // ray-refill kernel: flat ray space, rays per job, refill threshold
-    long long total_rays, rays_per_job;
-    int refill_threshold;
 };
 
 // Level table read through the read-only path (each warp may be on a
@@ -82,9 +85,12 @@ __global__ void batch_dem_kernel(const BatchDemSource *__restrict__ sources,
         fill_level(d.table, threadIdx.x, resolution, s.levels[threadIdx.x]);
 }
 
-template <bool kCount, bool kLadder>
-__global__ void __launch_bounds__(128, 8) march_sites_kernel(const __grid_constant__ SitesParams P) {
+template <bool kCount, int kLadder, int kMinBlocks>
+__global__ void __launch_bounds__(128, kMinBlocks)
+    march_sites_kernel(const __grid_constant__ SitesParams P) {
     const int lane = threadIdx.x & 31;
+    const int lanes = P.lanes_per_azimuth;
+    const int azimuths_per_job = 32 / lanes;
     unsigned visits = 0, samples = 0, steps = 0;
     for (;;) {
         unsigned long long taken = 0;
@@ -92,9 +98,12 @@ __global__ void __launch_bounds__(128, 8) march_sites_kernel(const __grid_consta
         const long long job = static_cast<long long>(__shfl_sync(0xffffffffu, taken, 0));
         if (job >= P.job_count) break;
         const int t = static_cast<int>(job / P.jobs_per_tile);
-        const long long linear = (job - t * P.jobs_per_tile) * 32 + lane;
-        const int pixel = static_cast<int>(linear % kTilePixels);
-        const int azimuth = static_cast<int>(linear / kTilePixels);
+        const long long local = job - t * P.jobs_per_tile;
+        const int azimuth_group = static_cast<int>(local / P.pixel_groups);
+        const int pixel_group = static_cast<int>(local - azimuth_group * P.pixel_groups);
+        const int pixel = pixel_group * lanes + lane % lanes;
+        const int azimuth = azimuth_group * azimuths_per_job + lane / lanes;
+        if (azimuth >= P.azimuth_count) continue;
         const BatchTile &tile = P.tiles[t];
         const int row = pixel / kTileSide, column = pixel % kTileSide;
         float *out = tile.out + static_cast<size_t>(pixel) * P.azimuth_count + azimuth;
@@ -129,132 +138,20 @@ __global__ void __launch_bounds__(128, 8) march_sites_kernel(const __grid_consta
     if (kCount) add_counters(P.counters, visits, samples, steps);
 }
 
-// The same march with dynamic ray fetching.  Rays of one warp finish at very
-// different times (with the skip ladder the longest of 32 adjacent rays does
-// about twice the mean work), so a lane whose ray (or DEM pass) ends does not
-// wait for the warp: once `refill_threshold` lanes wait, they take the next
-// rays of the warp's job (jobs of `rays_per_job` consecutive rays, taken from
-// the global counter) or begin their next pass, together, and every lane
-// then continues one march step at a time (march_step).  Per-ray arithmetic
-// is unchanged, so results equal the simple kernel's bit for bit.
-template <bool kCount, bool kLadder, int kMinBlocks>
-__global__ void __launch_bounds__(128, kMinBlocks)
-    march_sites_refill_kernel(const __grid_constant__ SitesParams P) {
-    const unsigned lane = threadIdx.x & 31;
-    const unsigned below = (1u << lane) - 1u;
-    const long long rays_per_tile = static_cast<long long>(kTilePixels) * P.azimuth_count;
-    long long pool_next = 0, pool_end = 0;  // warp-uniform
-    bool exhausted = false;                 // warp-uniform
-    enum { kIdle = 0, kBegin = 1, kMarch = 2 };
-    int phase = kIdle;
-    int t = 0, pixel = 0, azimuth = 0, d = 0, dem_count = 0;
-    float observer_z = 0.0f;
-    RaySegment g{};
-    DemView view{};
-    const LevelTable *table = nullptr;
-    MarchState st{0.0f, -1e30f, 0};
-    unsigned visits = 0, samples = 0, steps = 0;
-    for (;;) {
-        const unsigned waiting = __ballot_sync(0xffffffffu, phase != kMarch);
-        if (waiting == 0xffffffffu || __popc(waiting) >= P.refill_threshold) {
-            const unsigned idle = __ballot_sync(0xffffffffu, phase == kIdle);
-            if (idle != 0u) {
-                if (pool_next >= pool_end && !exhausted) {
-                    unsigned long long taken = 0;
-                    if (lane == 0) taken = atomicAdd(P.next_job, 1ull);
-                    const long long job =
-                        static_cast<long long>(__shfl_sync(0xffffffffu, taken, 0));
-                    const long long first = job * P.rays_per_job;
-                    if (first >= P.total_rays) {
-                        exhausted = true;
-                    } else {
-                        pool_next = first;
-                        pool_end = min(first + P.rays_per_job, P.total_rays);
-                    }
-                }
-                if (phase == kIdle) {
-                    const long long ray = pool_next + __popc(idle & below);
-                    if (ray < pool_end) {
-                        t = static_cast<int>(ray / rays_per_tile);
-                        const int r = static_cast<int>(ray - t * rays_per_tile);
-                        pixel = r % kTilePixels;
-                        azimuth = r / kTilePixels;
-                        const BatchTile &tile = P.tiles[t];
-                        const DemView &primary = P.dems[tile.dems[0]].view;
-                        const int row = pixel / kTileSide, column = pixel % kTileSide;
-                        if (tile.tile_column + column >= primary.width ||
-                            tile.tile_row + row >= primary.height) {
-                            // Outside the primary DEM: the -inf sentinel.
-                            tile.out[static_cast<size_t>(pixel) * P.azimuth_count + azimuth] =
-                                -INFINITY;
-                        } else {
-                            observer_z = __fadd_rn(
-                                bilinear(primary.cells, primary.width, primary.height,
-                                         static_cast<float>(tile.tile_column + column),
-                                         static_cast<float>(tile.tile_row + row)),
-                                tile.observer_elevation);
-                            d = 0;
-                            dem_count = tile.dem_count;
-                            st.current = -1e30f;
-                            phase = kBegin;
-                        }
-                    }
-                }
-                pool_next = min(pool_end, pool_next + __popc(idle));
-            }
-            if (phase == kBegin) {
-                const BatchTile &tile = P.tiles[t];
-                const DemView &primary = P.dems[tile.dems[0]].view;
-                const BatchDem &dem = P.dems[tile.dems[d]];
-                view = dem.view;
-                table = &dem.table;
-                const float ratio = __fdiv_rn(primary.column_res, view.column_res);
-                g = interpolate_segment(tile.segments, P.center_count, tile.dem_count, d,
-                                        azimuth, pixel % kTileSide, pixel / kTileSide,
-                                        tile.tile_column, tile.tile_row, kTileSide, P.subpatch,
-                                        primary.width, primary.height, ratio);
-                st = begin_pass(view, g, st.current);
-                phase = kMarch;
-            }
-            if (__ballot_sync(0xffffffffu, phase != kIdle) == 0u && exhausted &&
-                pool_next >= pool_end)
-                break;
-        }
-        if (phase == kMarch) {
-            if (!march_step<kCount, kLadder>(GlobalLevels{table}, view, g, d, observer_z, st,
-                                             visits, samples, steps)) {
-                if (++d < dem_count) {
-                    phase = kBegin;
-                } else {
-                    float value = st.current > -1e29f ? st.current : -INFINITY;
-                    if (P.degrees && !isinf(value)) value = __fmul_rn(atanf(value), kSlopeDegrees);
-                    P.tiles[t].out[static_cast<size_t>(pixel) * P.azimuth_count + azimuth] = value;
-                    phase = kIdle;
-                }
-            }
-        }
-    }
-    if (kCount) add_counters(P.counters, visits, samples, steps);
-}
-
-template <bool kCount, bool kLadder, int kMinBlocks>
-static void launch_refill(ls200_context *ctx, const SitesParams &P) {
-    int per_sm = 0;
-    LS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-        &per_sm, march_sites_refill_kernel<kCount, kLadder, kMinBlocks>, 128, 0));
-    const int blocks = ctx->props.multiProcessorCount * (per_sm > 0 ? per_sm : 1);
-    march_sites_refill_kernel<kCount, kLadder, kMinBlocks><<<blocks, 128, 0, ctx->stream>>>(P);
-    LS_CUDA(cudaGetLastError());
-}
-
-template <bool kCount, bool kLadder>
+template <bool kCount, int kLadder, int kMinBlocks>
 static void launch_sites(ls200_context *ctx, const SitesParams &P) {
     int per_sm = 0;
     LS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-        &per_sm, march_sites_kernel<kCount, kLadder>, 128, 0));
+        &per_sm, march_sites_kernel<kCount, kLadder, kMinBlocks>, 128, 0));
     const int blocks = ctx->props.multiProcessorCount * (per_sm > 0 ? per_sm : 1);
-    march_sites_kernel<kCount, kLadder><<<blocks, 128, 0, ctx->stream>>>(P);
+    march_sites_kernel<kCount, kLadder, kMinBlocks><<<blocks, 128, 0, ctx->stream>>>(P);
     LS_CUDA(cudaGetLastError());
+}
+
+template <bool kCount, int kMinBlocks>
+static void dispatch(ls200_context *ctx, const SitesParams &P, int traversal) {
+    if (traversal == kReference) launch_sites<kCount, kReference, kMinBlocks>(ctx, P);
+    else launch_sites<kCount, kLadderClimb, kMinBlocks>(ctx, P);
 }
 
 static size_t align_up(size_t n) { return (n + 255) & ~size_t(255); }
@@ -270,7 +167,8 @@ extern "C" ls200_status ls200_march_sites(ls200_context *ctx, const ls200_site_t
     return guard([&] {
         LS_REQUIRE(ctx && tiles && device_out, "NULL argument");
         LS_REQUIRE(tile_count > 0, "tile_count must be positive");
-        LS_REQUIRE(traversal == 0 || traversal == 1, "traversal must be 0 or 1");
+        LS_REQUIRE(traversal == kReference || traversal == kLadderClimb,
+                   "traversal must be 0 or 1");
         LS_REQUIRE(azimuth_count > 0 && static_cast<int64_t>(kTilePixels) * azimuth_count <
                                             (int64_t(1) << 31),
                    "azimuth_count is out of range");
@@ -378,40 +276,18 @@ extern "C" ls200_status ls200_march_sites(ls200_context *ctx, const ls200_site_t
         P.center_count = center_count;
         P.subpatch = subpatch_size;
         P.degrees = degrees ? 1 : 0;
-        P.jobs_per_tile = static_cast<long long>(kTilePixels) * azimuth_count / 32;
+        P.lanes_per_azimuth = ctx->batch_lanes_per_azimuth;
+        const int azimuths_per_job = 32 / P.lanes_per_azimuth;
+        P.pixel_groups = kTilePixels / P.lanes_per_azimuth;
+        P.jobs_per_tile = P.pixel_groups * ((azimuth_count + azimuths_per_job - 1) /
+                                            azimuths_per_job);
         P.job_count = P.jobs_per_tile * tile_count;
         P.next_job = reinterpret_cast<unsigned long long *>(scratch + off_job);
         P.counters = ctx->counters.as<unsigned long long>();
-        P.total_rays = static_cast<long long>(kTilePixels) * azimuth_count * tile_count;
-        P.rays_per_job = ctx->batch_rays_per_job;
-        P.refill_threshold = ctx->batch_refill;
         reset_counters(ctx);
-        const bool ladder = traversal != 0;
-        if (ctx->batch_kernel == 0) {
-            if (ctx->counting) {
-                if (ladder) launch_sites<true, true>(ctx, P);
-                else launch_sites<true, false>(ctx, P);
-            } else {
-                if (ladder) launch_sites<false, true>(ctx, P);
-                else launch_sites<false, false>(ctx, P);
-            }
-        } else if (ctx->batch_min_blocks == 6) {
-            if (ctx->counting) {
-                if (ladder) launch_refill<true, true, 6>(ctx, P);
-                else launch_refill<true, false, 6>(ctx, P);
-            } else {
-                if (ladder) launch_refill<false, true, 6>(ctx, P);
-                else launch_refill<false, false, 6>(ctx, P);
-            }
-        } else {
-            if (ctx->counting) {
-                if (ladder) launch_refill<true, true, 8>(ctx, P);
-                else launch_refill<true, false, 8>(ctx, P);
-            } else {
-                if (ladder) launch_refill<false, true, 8>(ctx, P);
-                else launch_refill<false, false, 8>(ctx, P);
-            }
-        }
+        if (ctx->counting) dispatch<true, 8>(ctx, P, traversal);
+        else if (ctx->batch_min_blocks == 6) dispatch<false, 6>(ctx, P, traversal);
+        else dispatch<false, 8>(ctx, P, traversal);
         if (seconds) LS_CUDA(cudaEventRecord(ctx->events[2], ctx->stream));
         // The host tables above must outlive their copies.
         LS_CUDA(cudaStreamSynchronize(ctx->stream));
@@ -426,31 +302,26 @@ extern "C" ls200_status ls200_march_sites(ls200_context *ctx, const ls200_site_t
     });
 }
 
-extern "C" ls200_status ls200_set_batch_config(ls200_context *ctx, int kernel, int refill,
-                                               int rays_per_job, int min_blocks) {
+extern "C" ls200_status ls200_set_batch_config(ls200_context *ctx, int lanes_per_azimuth,
+                                               int min_blocks) {
     return guard([&] {
         LS_REQUIRE(ctx, "NULL argument");
-        LS_REQUIRE(kernel == 0 || kernel == 1, "kernel must be 0 or 1");
-        LS_REQUIRE(refill >= 1 && refill <= 32, "refill threshold must be between 1 and 32");
-        LS_REQUIRE(rays_per_job >= 32 && rays_per_job % 32 == 0 && rays_per_job <= (1 << 20),
-                   "rays_per_job must be a multiple of 32 up to 2^20");
+        LS_REQUIRE(lanes_per_azimuth >= 1 && lanes_per_azimuth <= 32 &&
+                       (lanes_per_azimuth & (lanes_per_azimuth - 1)) == 0,
+                   "lanes_per_azimuth must be a power of two from 1 to 32");
         LS_REQUIRE(min_blocks == 6 || min_blocks == 8, "min_blocks must be 6 or 8");
         std::lock_guard<std::mutex> hold(ctx->lock);
-        ctx->batch_kernel = kernel;
-        ctx->batch_refill = refill;
-        ctx->batch_rays_per_job = rays_per_job;
+        ctx->batch_lanes_per_azimuth = lanes_per_azimuth;
         ctx->batch_min_blocks = min_blocks;
     });
 }
 
-extern "C" ls200_status ls200_get_batch_config(ls200_context *ctx, int *kernel, int *refill,
-                                               int *rays_per_job, int *min_blocks) {
+extern "C" ls200_status ls200_get_batch_config(ls200_context *ctx, int *lanes_per_azimuth,
+                                               int *min_blocks) {
     return guard([&] {
-        LS_REQUIRE(ctx && kernel && refill && rays_per_job && min_blocks, "NULL argument");
+        LS_REQUIRE(ctx && lanes_per_azimuth && min_blocks, "NULL argument");
         std::lock_guard<std::mutex> hold(ctx->lock);
-        *kernel = ctx->batch_kernel;
-        *refill = ctx->batch_refill;
-        *rays_per_job = ctx->batch_rays_per_job;
+        *lanes_per_azimuth = ctx->batch_lanes_per_azimuth;
         *min_blocks = ctx->batch_min_blocks;
     });
 }

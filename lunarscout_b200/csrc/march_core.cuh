@@ -265,36 +265,82 @@ __device__ __forceinline__ float cell_exit_advance(int shift, int cx, int cy, fl
 // distance, so the bound is the slope formula at d0; with dh < 0 every slope
 // is below dh / d1 (the curvature drop only lowers it).  The cull needs the
 // bound below `current` by a relative 4e-6, which covers its rounding.
+//
+// The decision is made on a cheap approximation of the bound whenever it lies
+// outside a guard band around `current` (as in bound_culled: the far-field
+// approximation is within 2e-6 relative of the exact float32 bound, the
+// divisions within 2 ulp; the band is 1e-5 relative), and with the exact
+// arithmetic inside it, so the decision is always that of the exact test.
+// ladder_culled tests the level-m ancestor and sets `step` to its exit
+// advance; ladder_advance climbs from `level`, returns the advance and sets
+// `reached` to the largest culled level (`level` if none).
+template <class Table>
+__device__ __forceinline__ bool ladder_culled(const Table &table, const float *__restrict__ cells,
+                                              int m, int ipx, int ipy, float px, float py,
+                                              float inv_x, float inv_y, bool near, float true_m,
+                                              float radius, float observer_z,
+                                              float observer_radius, float inverse_denominator,
+                                              float current, float &step) {
+    const int shift = 2 * m;
+    const int cx = ipx >> shift, cy = ipy >> shift;
+    const float maximum_height = four_cell_bound(cells, table.cells(m), cx, cy);
+    step = cell_exit_advance(shift, cx, cy, px, py, inv_x, inv_y, table.fallback(m));
+    if (maximum_height < -20000.0f) return true;
+    const float dh = __fsub_rn(maximum_height, observer_z);
+    const float far_distance = __fadd_rn(__fadd_rn(true_m, __fmul_rn(step, 1010.0f)), 1.0f);
+    float approx;
+    bool exact = false;
+    if (dh < 0.0f) {
+        approx = __fdividef(dh, far_distance);
+    } else if (near) {
+        approx = __fdividef(dh, true_m);
+    } else {
+        const float squared = __fmul_rn(true_m, true_m);
+        float radius_sum = __fadd_rn(__fmul_rn(2.0f, radius), maximum_height);
+        radius_sum = __fadd_rn(radius_sum, observer_z);
+        const float numerator = __fmaf_rn(dh, radius_sum, -squared);
+        const float local_z = __fmul_rn(numerator, inverse_denominator);
+        const float lx2 = __fmaf_rn(true_m, true_m, -__fmul_rn(local_z, local_z));
+        exact = !(lx2 > 0.25f * squared);
+        approx = exact ? 0.0f : __fmul_rn(local_z, rsqrtf(lx2));
+    }
+    if (!exact) {
+        const float size = fmaxf(fabsf(approx), fabsf(current));
+        const float decided = __fadd_rn(approx, __fmul_rn(4e-6f, size));
+        const float band = 1e-5f * size + 1e-30f;
+        if (decided < current - band) return true;
+        if (decided > current + band) return false;
+    }
+    float bound;
+    if (dh < 0.0f) {
+        bound = __fdiv_rn(dh, far_distance);
+    } else {
+        bound = near ? __fdiv_rn(dh, true_m)
+                     : bound_slope(true_m, maximum_height, radius, observer_z, observer_radius);
+    }
+    const float size = fmaxf(fabsf(bound), fabsf(current));
+    return __fadd_rn(bound, __fmul_rn(4e-6f, size)) <= current;
+}
+
 template <bool kCount, class Table>
 __device__ __forceinline__ float ladder_advance(const Table &table, const float *__restrict__ cells,
                                                 int level, int top, int ipx, int ipy, float px,
                                                 float py, float inv_x, float inv_y, bool near,
                                                 float true_m, float radius, float observer_z,
-                                                float observer_radius, float current,
-                                                float advance, unsigned &visits) {
+                                                float observer_radius, float inverse_denominator,
+                                                float current, float advance, unsigned &visits,
+                                                int &reached) {
+    reached = level;
     if (true_m < kLadderMinimumDistance) return advance;
     float best = advance;
     for (int m = level + 1; m <= top; ++m) {
-        const int shift = 2 * m;
-        const int cx = ipx >> shift, cy = ipy >> shift;
-        const float maximum_height = four_cell_bound(cells, table.cells(m), cx, cy);
-        const float step =
-            cell_exit_advance(shift, cx, cy, px, py, inv_x, inv_y, table.fallback(m));
+        float step;
         if (kCount) ++visits;
-        if (!(maximum_height < -20000.0f)) {
-            const float dh = __fsub_rn(maximum_height, observer_z);
-            float bound;
-            if (dh >= 0.0f) {
-                bound = near ? __fdiv_rn(dh, true_m)
-                             : bound_slope(true_m, maximum_height, radius, observer_z,
-                                           observer_radius);
-            } else {
-                bound = __fdiv_rn(dh, __fadd_rn(__fadd_rn(true_m, __fmul_rn(step, 1010.0f)), 1.0f));
-            }
-            const float size = fmaxf(fabsf(bound), fabsf(current));
-            if (!(__fadd_rn(bound, __fmul_rn(4e-6f, size)) <= current)) break;
-        }
+        if (!ladder_culled(table, cells, m, ipx, ipy, px, py, inv_x, inv_y, near, true_m, radius,
+                           observer_z, observer_radius, inverse_denominator, current, step))
+            break;
         best = step;
+        reached = m;
     }
     return best;
 }
@@ -378,11 +424,14 @@ __device__ __forceinline__ MarchState begin_pass(const DemView &dem, const RaySe
     return MarchState{g.s_start > 0.001f ? g.s_start : 0.001f, current, dem.level_count - 1};
 }
 
+// Traversals of march_step: the reference's, and the skip ladder.
+enum Traversal { kReference = 0, kLadderClimb = 1 };
+
 // One outer iteration of hierarchy_maximum (cuda_backend.py:672-867): one ray
-// position, the level descent (and with kLadder the climb) and the advance.
+// position, the level descent (and with the ladder the climb) and the advance.
 // Returns false, leaving `st` untouched, when the pass is over (past s_end,
 // outside the DEM, or the cell left the level grid).
-template <bool kCount, bool kLadder, class Table>
+template <bool kCount, int kLadder, class Table>
 __device__ __forceinline__ bool march_step(const Table &table, const DemView &dem,
                                            const RaySegment &g, int pass_index,
                                            float observer_z, MarchState &st, unsigned &visits,
@@ -461,11 +510,13 @@ __device__ __forceinline__ bool march_step(const Table &table, const DemView &de
             }
             if (culled) {
                 float advance = skip;
-                if (kLadder) {
+                if (kLadder != kReference) {
+                    int reached;
                     advance = ladder_advance<kCount>(table, cells, level, top_level, ipx, ipy,
                                                      px, py, inv_x, inv_y, near, true_m, radius,
-                                                     observer_z, observer_radius, current, skip,
-                                                     visits);
+                                                     observer_z, observer_radius,
+                                                     inverse_denominator, current, skip, visits,
+                                                     reached);
                 }
                 s = __fadd_rn(s, advance);
                 break;
@@ -481,13 +532,20 @@ __device__ __forceinline__ bool march_step(const Table &table, const DemView &de
                 }
                 const float magnitude = hypot_fused(dx, dy);
                 const float pixel_step = magnitude > 1e-6f ? __frcp_rn(magnitude) : 0.0005f;
+                // inner = min(margin_step, angular_step), both a product
+                // divided by 1000 (the margin one 0 unless margin > 0).  A
+                // correctly rounded division by a positive constant is
+                // monotone, so the smaller quotient is the quotient of the
+                // smaller product: one division gives the same value.
                 const float margin = __fsub_rn(current, slope);
-                const float margin_step =
-                    margin > 0.0f
-                        ? __fdiv_rn(__fmul_rn(__fmul_rn(margin, true_m), 1.732f), 1000.0f)
-                        : 0.0f;
-                const float angular_step = __fdiv_rn(__fmul_rn(true_m, 0.00151f), 1000.0f);
-                const float inner = margin_step < angular_step ? margin_step : angular_step;
+                const float angular_product = __fmul_rn(true_m, 0.00151f);
+                float inner = 0.0f;
+                if (margin > 0.0f) {
+                    const float margin_product = __fmul_rn(__fmul_rn(margin, true_m), 1.732f);
+                    inner = __fdiv_rn(margin_product < angular_product ? margin_product
+                                                                       : angular_product,
+                                      1000.0f);
+                }
                 float advance = pixel_step > inner ? pixel_step : inner;
                 if (near) advance = __fmul_rn(advance, 0.25f);
                 const float floor_step =
@@ -509,7 +567,7 @@ __device__ __forceinline__ bool march_step(const Table &table, const DemView &de
 // hierarchy_maximum (cuda_backend.py:656-874): the maximum slope along one
 // ray over one DEM, starting from `current` (-1e30 for none).  Table gives
 // side(l), fallback(l), out_step(l) and cells(l).
-template <bool kCount, bool kLadder, class Table>
+template <bool kCount, int kLadder, class Table>
 __device__ __forceinline__ float march_dem(const Table &table, const DemView &dem,
                                            const RaySegment &g, int pass_index,
                                            float observer_z, float current, unsigned &visits,

@@ -49,14 +49,12 @@ class SiteTile:
 
 @dataclass(frozen=True, slots=True)
 class BatchConfig:
-    """Launch configuration of the persistent multi-site march: ``kernel`` 0
-    (one ray per lane) or 1 (dynamic ray fetching), the ``refill`` threshold
-    (waiting lanes of 32), ``rays_per_job`` taken per work-counter increment,
-    and ``min_blocks`` resident 128-thread blocks per SM (8 or 6)."""
+    """Launch configuration of the persistent multi-site march:
+    ``lanes_per_azimuth`` adjacent pixels of one azimuth per 32-ray warp job
+    (a power of two up to 32; the job spans 32/lanes azimuths) and ``min_blocks``
+    resident 128-thread blocks per SM (8 at 64 registers or 6 at 80)."""
 
-    kernel: int = 1
-    refill: int = 8
-    rays_per_job: int = 128
+    lanes_per_azimuth: int = 32
     min_blocks: int = 8
 
 
@@ -379,11 +377,11 @@ class CudaSession:
 
     def set_batch_config(self, config: BatchConfig) -> None:
         """Launch configuration of :meth:`march_sites` (results do not depend on it)."""
-        call("ls200_set_batch_config", self._ctx, int(config.kernel), int(config.refill),
-             int(config.rays_per_job), int(config.min_blocks))
+        call("ls200_set_batch_config", self._ctx, int(config.lanes_per_azimuth),
+             int(config.min_blocks))
 
     def batch_config(self) -> BatchConfig:
-        values = [ctypes.c_int() for _ in range(4)]
+        values = [ctypes.c_int() for _ in range(2)]
         call("ls200_get_batch_config", self._ctx, *[ctypes.byref(v) for v in values])
         return BatchConfig(*(v.value for v in values))
 

@@ -39,14 +39,13 @@ def _fake_run(times):
 def test_default_candidates_are_valid_and_unique():
     assert len(set(DEFAULT_CANDIDATES)) == len(DEFAULT_CANDIDATES)
     for config in DEFAULT_CANDIDATES:
-        assert config.kernel in (0, 1)
-        assert 1 <= config.refill <= 32
-        assert config.rays_per_job % 32 == 0
+        assert config.lanes_per_azimuth in (32, 16, 8, 4, 2, 1)
         assert config.min_blocks in (6, 8)
+    assert DEFAULT_CANDIDATES[0] == BatchConfig()
 
 
 def test_select_best_prefers_the_fastest_then_the_earliest():
-    a, b, c = BatchConfig(0), BatchConfig(1, 4), BatchConfig(1, 16)
+    a, b, c = BatchConfig(32), BatchConfig(16), BatchConfig(8)
     assert select_best({a: 2.0, b: 1.0, c: 3.0}, (a, b, c)) == b
     assert select_best({a: 1.0, b: 1.0}, (b, a)) == b
     with pytest.raises(ValueError):
@@ -61,7 +60,7 @@ def test_tune_applies_the_winner_or_restores_the_previous():
     result = tune_batch(session, [object()] * 3, device_out=0, run=_fake_run(times))
     assert result.best == winner and session.config == winner
     assert set(result.seconds) == set(DEFAULT_CANDIDATES)
-    before = BatchConfig(1, 16, 512, 6)
+    before = BatchConfig(8, 6)
     session.set_batch_config(before)
     tune_batch(session, [object()], device_out=0, run=_fake_run(times), apply=False)
     assert session.config == before
@@ -69,14 +68,14 @@ def test_tune_applies_the_winner_or_restores_the_previous():
 
 def test_tune_restores_the_configuration_when_a_run_fails():
     session = FakeSession()
-    session.set_batch_config(BatchConfig(0, 8, 128, 8))
+    session.set_batch_config(BatchConfig(16, 8))
 
     def broken(sess, tiles):
         raise RuntimeError("launch failed")
 
     with pytest.raises(RuntimeError):
         tune_batch(session, [object()], device_out=0, run=broken)
-    assert session.config == BatchConfig(0, 8, 128, 8)
+    assert session.config == BatchConfig(16, 8)
 
 
 def test_cache_round_trip(tmp_path):

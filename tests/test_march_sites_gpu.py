@@ -106,7 +106,8 @@ def test_ladder_traversal_equals_its_cpu_restatement(batch, cuda_session):
                                           projection_parameters(dem)))
         expected, _ = oracle.march_all_passes(
             segments, pyramids, tile_column=tile.tile_column, tile_row=tile.tile_row,
-            observer_elevation_m=tile.observer_elevation_m, mask=oracle.ladder_mask(0, 1))
+            observer_elevation_m=tile.observer_elevation_m,
+            mask=oracle.ladder_mask(0, 1))
         np.testing.assert_array_equal(got[t], expected, err_msg=f"tile {t}")
 
 
@@ -193,7 +194,7 @@ def test_autotuner_times_every_candidate_and_applies_the_winner(batch, cuda_sess
     finally:
         cuda_session.set_batch_config(default)
     with pytest.raises(ValueError):
-        cuda_session.set_batch_config(BatchConfig(1, 8, 100, 8))
+        cuda_session.set_batch_config(BatchConfig(12, 8))
     with pytest.raises(ValueError):
-        cuda_session.set_batch_config(BatchConfig(1, 8, 128, 7))
+        cuda_session.set_batch_config(BatchConfig(32, 7))
     assert cuda_session.batch_config() == default

@@ -75,6 +75,12 @@ ls200_status ls200_dem_create(ls200_context *ctx, const float *level0, int width
 ls200_status ls200_dem_destroy(ls200_dem *dem);
 /* Copies the device mips back (e.g. to write a .pyr.bin cache). */
 ls200_status ls200_dem_download_mips(ls200_dem *dem, float *mips, int64_t capacity);
+/* Replace the DEM's heights from device memory (width*height float32) and
+ * rebuild its pyramid on the device: the differentiable path's way of
+ * marching a DEM held in a framework tensor.  No reference counterpart. */
+ls200_status ls200_dem_set_heights_device(ls200_dem *dem, const float *device_heights);
+/* Device address of the DEM's (raw) level-0 heights. */
+ls200_status ls200_dem_level0_device(ls200_dem *dem, const float **device_level0);
 
 /* ---- ray segments: src/lunarscout/_numba_horizon/geometry.py:575-673
  *      (build_subpatch_segments_numba) and geometry_numba.py:142-364 ---- */
@@ -254,6 +260,33 @@ ls200_status ls200_sun_fraction(ls200_context *ctx, const float *horizons,
 /* Page-locked host memory for H2D/D2H staging (cudaHostAlloc). */
 ls200_status ls200_host_alloc(int64_t bytes, void **out);
 ls200_status ls200_host_free(void *ptr);
+
+/* ---- DEM adjoint of a time-integrated sun fraction (no reference
+ *      counterpart; the interpolation of the horizon at the sun azimuth is
+ *      nh/lightmap_cuda.py:125-145's) ----
+ * loss = sum over tiles, pixels of w * mean over the `sun` vectors of
+ * F((el - h) / r): F = visible fraction of a disk of radius r (degrees)
+ * above a level horizon line, h = the horizon (degrees, clamped at -90)
+ * interpolated at the sun azimuth.  Every tile must use the same DEM stack.
+ * The forward marches the tiles (ls200_march_sites, `traversal` 0 or 1) with
+ * one checkpoint per ray (the winning sample) kept in the context for the
+ * next backward; device_weights holds tile_count x 16384 float32.  seconds
+ * (may be NULL) gets {march, lighting + loss}.  The backward adds
+ * grad_output * dloss/dheight into device_grads[d] (float64 [H_d, W_d], one
+ * per DEM of the stack, accumulated); *seconds (may be NULL) its time. */
+ls200_status ls200_sun_loss_forward(ls200_context *ctx, const ls200_site_tile *tiles,
+                                    int tile_count, int azimuth_count, int traversal,
+                                    const float *device_weights, const ls200_vectors *sun,
+                                    double disk_radius_deg, double *loss, double *seconds);
+ls200_status ls200_sun_loss_backward(ls200_context *ctx, double grad_output,
+                                     double *const *device_grads, int grad_count,
+                                     double *seconds);
+/* Host copies of the last forward's checkpoints (rays x 4 float: px, py,
+ * distance m, slope; flags = pass << 1 | near, 0xff for none), sun
+ * directions ([tiles, T, 16384] x (azimuth, elevation) degrees) and horizons
+ * (degrees); any pointer may be NULL. */
+ls200_status ls200_sun_loss_checkpoints(ls200_context *ctx, float *points, uint8_t *flags,
+                                        float *directions, float *horizons);
 
 /* FP32 FMA issue-rate probe (TFLOP/s, 2 flops per FMA) on this device: the
  * measured denominator of the march's FP32 roofline.  No reference

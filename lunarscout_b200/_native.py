@@ -87,6 +87,11 @@ SIGNATURES: dict[str, list] = {
     "ls200_slopes_to_degrees": [_vp, _f32p, _i64, _f32p],
     "ls200_horizon_tile": [_vp, _vp, _i, _i, _i, _i, _d, _f, _i, _i, _vp, _i64, _vp],
     "ls200_march_sites": [_vp, _vp, _i, _i, _i, _i, _i, _vp, _vp],
+    "ls200_dem_set_heights_device": [_vp, _vp],
+    "ls200_dem_level0_device": [_vp, _vp],
+    "ls200_sun_loss_forward": [_vp, _vp, _i, _i, _i, _vp, _vp, _d, _vp, _vp],
+    "ls200_sun_loss_backward": [_vp, _d, _vp, _i, _vp],
+    "ls200_sun_loss_checkpoints": [_vp, _vp, _vp, _vp, _vp],
     "ls200_set_batch_config": [_vp, _i, _i],
     "ls200_get_batch_config": [_vp, _vp, _vp],
     "ls200_cbin_encode": [_vp, _f32p, _vp, _i64, _vp],

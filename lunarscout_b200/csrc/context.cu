@@ -97,6 +97,7 @@ ls200_status ls200_context_destroy(ls200_context *ctx) {
         ctx->dems.clear();
         release_lighting_state(ctx);
         release_codec(ctx);
+        release_adjoint_state(ctx);
         for (auto &event : ctx->events)
             if (event) cudaEventDestroy(event);
         if (ctx->own_stream) cudaStreamDestroy(ctx->own_stream);
@@ -251,6 +252,28 @@ ls200_status ls200_build_max_pyramid(ls200_context *ctx, const float *level0, in
     s = ls200_dem_download_mips(dem, mips, dem->mip_count);
     ls200_status t = ls200_dem_destroy(dem);
     return s != LS200_OK ? s : t;
+}
+
+ls200_status ls200_dem_set_heights_device(ls200_dem *dem, const float *device_heights) {
+    return guard([&] {
+        LS_REQUIRE(dem && device_heights, "NULL argument");
+        ls200_context *ctx = dem->ctx;
+        std::lock_guard<std::mutex> hold(ctx->lock);
+        activate(ctx);
+        LS_CUDA(cudaMemcpyAsync(dem->level0, device_heights,
+                                sizeof(float) * size_t(dem->width) * dem->height,
+                                cudaMemcpyDeviceToDevice, ctx->stream));
+        build_pyramid_device(ctx, dem);
+        sanitize_level0(ctx, dem);
+        LS_CUDA(cudaStreamSynchronize(ctx->stream));
+    });
+}
+
+ls200_status ls200_dem_level0_device(ls200_dem *dem, const float **device_level0) {
+    return guard([&] {
+        LS_REQUIRE(dem && device_level0, "NULL argument");
+        *device_level0 = dem->level0;
+    });
 }
 
 ls200_status ls200_set_counting(ls200_context *ctx, int enabled) {

@@ -91,6 +91,7 @@ struct PyramidLevel {
 
 struct LightingState;  // lighting tile buffers of a context (lighting_api.cu)
 struct CodecBuffers;   // .cbin codec buffers of a context (codec.cu)
+struct AdjointState;   // checkpoints of the last sun-loss forward (adjoint.cu)
 
 }  // namespace ls200
 
@@ -127,6 +128,7 @@ struct ls200_context {
     std::set<ls200_dem *> dems;  // live DEMs, released with the context
     ls200::LightingState *lighting = nullptr;
     ls200::CodecBuffers *codec = nullptr;
+    ls200::AdjointState *adjoint = nullptr;
     // Launch configuration of the persistent multi-site march.
     int batch_lanes_per_azimuth = 32;  // pixels of one azimuth in a 32-ray job (1..32)
     int batch_min_blocks = 8;          // resident 128-thread blocks per SM (8 or 6)
@@ -141,6 +143,8 @@ void activate(ls200_context *ctx);
 void release_lighting_state(ls200_context *ctx);
 // Free the codec buffers owned by a context.
 void release_codec(ls200_context *ctx);
+// Free the adjoint checkpoints owned by a context.
+void release_adjoint_state(ls200_context *ctx);
 // .cbin-encode device degrees [16384, 1440] into device `payload` (capacity
 // >= 16384 * 2882 bytes) on ctx->stream; returns the size (synchronises).
 int64_t cbin_encode(ls200_context *ctx, const float *degrees, uint8_t *payload);
@@ -171,6 +175,15 @@ struct MarchTile {
 void march_pass_device(ls200_context *ctx, const MarchTile &tile, const ls200_dem *primary,
                        const ls200_dem *active, int pass_index, bool first_pass,
                        float *slopes_az_major);
+
+// The persistent multi-site march (march_batch.cu): validates, takes the
+// context lock, builds segments and marches every tile into device_out
+// ([tile_count, 16384, A]); with `checkpoints` it also records each ray's
+// winning sample (see SitesParams) for the DEM adjoint.
+void march_sites_run(ls200_context *ctx, const ls200_site_tile *tiles, int tile_count,
+                     int azimuth_count, int subpatch_size, int traversal, bool degrees,
+                     float *device_out, double *seconds, float4 *checkpoints,
+                     uint8_t *checkpoint_flags);
 
 // Zero the march counters before a counted launch / read them back after it
 // (both no-ops unless counting is enabled).

@@ -221,6 +221,43 @@ void lighting_launch(ls200_context *ctx, LightingBatch &B, int tiles, int signal
     LS_CUDA(cudaGetLastError());
 }
 
+__global__ void __launch_bounds__(128) directions_kernel(const __grid_constant__ LightingBatch B,
+                                                         float2 *__restrict__ out) {
+    const int tile = blockIdx.z;
+    const int index = blockIdx.x * blockDim.x + threadIdx.x;
+    if (index >= kPatch * kPatch) return;
+    const TileGeo &g = B.tiles[tile];
+    const int sample = index % kPatch, line = index / kPatch;
+    const int t0 = B.time_start + blockIdx.y * B.chunk;
+    const int t1 = min(t0 + B.chunk, B.time_start + B.time_count);
+    const size_t plane = static_cast<size_t>(kPatch) * kPatch;
+    const size_t tile_out = static_cast<size_t>(tile) * B.time_count * plane;
+    const bool valid = sample < g.valid_width && line < g.valid_height;
+    Frame32 f;
+    const float *src = B.frames + (static_cast<size_t>(tile) * plane + index) * 12;
+#pragma unroll
+    for (int k = 0; k < 12; ++k) f.v[k] = src[k];
+    for (int t = t0; t < t1; ++t) {
+        float2 direction = make_float2(0.0f, 0.0f);
+        if (valid) {
+            const float *v = B.vectors + 3 * static_cast<size_t>(t);
+            body_direction(f, __ldg(v), __ldg(v + 1), __ldg(v + 2), direction.x, direction.y);
+        }
+        out[tile_out + static_cast<size_t>(t - B.time_start) * plane + index] = direction;
+    }
+}
+
+void directions_launch(ls200_context *ctx, LightingBatch &B, int tiles, float2 *out) {
+    LS_REQUIRE(tiles >= 1 && tiles <= kMaxBatchTiles, "1 to 32 tiles per launch");
+    dim3 grid_frames(kPatch * kPatch / 128, tiles);
+    frames_kernel<<<grid_frames, 128, 0, ctx->stream>>>(B);
+    LS_CUDA(cudaGetLastError());
+    B.chunk = lighting_chunk(ctx, tiles, B.time_count);
+    dim3 grid(kPatch * kPatch / 128, (B.time_count + B.chunk - 1) / B.chunk, tiles);
+    directions_kernel<<<grid, 128, 0, ctx->stream>>>(B, out);
+    LS_CUDA(cudaGetLastError());
+}
+
 void sun_fraction_launch(ls200_context *ctx, const float *horizons, const float *azimuth_deg,
                          const float *elevation_deg, int n, float *out) {
     ensure_lighting_constants(ctx);

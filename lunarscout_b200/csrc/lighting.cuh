@@ -6,6 +6,13 @@
 
 #include "internal.cuh"
 
+// A Moon-ME vector table resident on the device (ls200_vectors_create).
+struct ls200_vectors {
+    ls200_context *ctx = nullptr;
+    float *data = nullptr;  // device [count, 3]
+    int count = 0;
+};
+
 namespace ls200 {
 
 constexpr int kPatch = 128;
@@ -37,6 +44,10 @@ void lighting_launch(ls200_context *ctx, LightingBatch &batch, int tiles, int si
 void sun_fraction_launch(ls200_context *ctx, const float *horizons, const float *azimuth_deg,
                          const float *elevation_deg, int n, float *out);
 void ensure_lighting_constants(ls200_context *ctx);
+// Per-pixel frames of the batch's tiles, then the Sun's (azimuth deg,
+// elevation deg) at every pixel and time step of [time_start, +time_count):
+// out [tiles, time_count, 16384] (zero outside the valid rectangle).
+void directions_launch(ls200_context *ctx, LightingBatch &batch, int tiles, float2 *out);
 
 #ifdef LS200_LIGHTING_KERNELS
 // Slice half-heights and their normaliser (set by ensure_lighting_constants).

@@ -1,12 +1,6 @@
 // C-ABI entry points of the lighting products.
 #include "lighting.cuh"
 
-struct ls200_vectors {
-    ls200_context *ctx = nullptr;
-    float *data = nullptr;  // device [count, 3]
-    int count = 0;
-};
-
 namespace ls200 {
 
 struct LightingState {

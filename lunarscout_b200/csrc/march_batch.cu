@@ -61,6 +61,11 @@ struct SitesParams {
     long long pixel_groups, jobs_per_tile, job_count;
     unsigned long long *next_job;
     unsigned long long *counters;
+    // Adjoint checkpoints (NULL when not recorded), per ray like `out`:
+    // (px, py, true_m, slope) of the winning level-0 sample, and
+    // flags = pass << 1 | near (0xff when no sample won).
+    float4 *checkpoints;
+    uint8_t *checkpoint_flags;
 };
 
 // Level table read through the read-only path (each warp may be on a
@@ -85,7 +90,16 @@ __global__ void batch_dem_kernel(const BatchDemSource *__restrict__ sources,
         fill_level(d.table, threadIdx.x, resolution, s.levels[threadIdx.x]);
 }
 
-template <bool kCount, int kLadder, int kMinBlocks>
+template <bool kArgmax>
+struct TrackerOf {
+    using type = NoArgmax;
+};
+template <>
+struct TrackerOf<true> {
+    using type = Argmax;
+};
+
+template <bool kCount, int kLadder, int kMinBlocks, bool kArgmax = false>
 __global__ void __launch_bounds__(128, kMinBlocks)
     march_sites_kernel(const __grid_constant__ SitesParams P) {
     const int lane = threadIdx.x & 31;
@@ -106,12 +120,16 @@ __global__ void __launch_bounds__(128, kMinBlocks)
         if (azimuth >= P.azimuth_count) continue;
         const BatchTile &tile = P.tiles[t];
         const int row = pixel / kTileSide, column = pixel % kTileSide;
-        float *out = tile.out + static_cast<size_t>(pixel) * P.azimuth_count + azimuth;
+        const size_t ray = static_cast<size_t>(pixel) * P.azimuth_count + azimuth;
+        float *out = tile.out + ray;
         const BatchDem &primary = P.dems[tile.dems[0]];
         const int primary_width = primary.view.width, primary_height = primary.view.height;
+        typename TrackerOf<kArgmax>::type tracker;
+        const size_t checkpoint = static_cast<size_t>(t) * kTilePixels * P.azimuth_count + ray;
         // Pixels outside the primary DEM keep the -inf sentinel.
         if (tile.tile_column + column >= primary_width || tile.tile_row + row >= primary_height) {
             *out = -INFINITY;
+            if (kArgmax) P.checkpoint_flags[checkpoint] = 0xff;
             continue;
         }
         const float observer_z = __fadd_rn(
@@ -128,8 +146,17 @@ __global__ void __launch_bounds__(128, kMinBlocks)
                 tile.segments, P.center_count, tile.dem_count, d, azimuth, column, row,
                 tile.tile_column, tile.tile_row, kTileSide, P.subpatch, primary_width,
                 primary_height, ratio);
-            current = march_dem<kCount, kLadder>(GlobalLevels{&dem.table}, view, g, d, observer_z,
-                                                 current, visits, samples, steps);
+            if constexpr (kArgmax) tracker.current_pass = d;
+            current = march_dem_tracked<kCount, kLadder>(GlobalLevels{&dem.table}, view, g, d,
+                                                         observer_z, current, visits, samples,
+                                                         steps, tracker);
+        }
+        if constexpr (kArgmax) {
+            P.checkpoints[checkpoint] =
+                make_float4(tracker.px, tracker.py, tracker.true_m, tracker.slope);
+            P.checkpoint_flags[checkpoint] =
+                tracker.pass < 0 ? uint8_t(0xff)
+                                 : static_cast<uint8_t>((tracker.pass << 1) | tracker.near);
         }
         float value = current > -1e29f ? current : -INFINITY;
         if (P.degrees && !isinf(value)) value = __fmul_rn(atanf(value), kSlopeDegrees);
@@ -138,13 +165,13 @@ __global__ void __launch_bounds__(128, kMinBlocks)
     if (kCount) add_counters(P.counters, visits, samples, steps);
 }
 
-template <bool kCount, int kLadder, int kMinBlocks>
+template <bool kCount, int kLadder, int kMinBlocks, bool kArgmax = false>
 static void launch_sites(ls200_context *ctx, const SitesParams &P) {
     int per_sm = 0;
     LS_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
-        &per_sm, march_sites_kernel<kCount, kLadder, kMinBlocks>, 128, 0));
+        &per_sm, march_sites_kernel<kCount, kLadder, kMinBlocks, kArgmax>, 128, 0));
     const int blocks = ctx->props.multiProcessorCount * (per_sm > 0 ? per_sm : 1);
-    march_sites_kernel<kCount, kLadder, kMinBlocks><<<blocks, 128, 0, ctx->stream>>>(P);
+    march_sites_kernel<kCount, kLadder, kMinBlocks, kArgmax><<<blocks, 128, 0, ctx->stream>>>(P);
     LS_CUDA(cudaGetLastError());
 }
 
@@ -154,17 +181,18 @@ static void dispatch(ls200_context *ctx, const SitesParams &P, int traversal) {
     else launch_sites<kCount, kLadderClimb, kMinBlocks>(ctx, P);
 }
 
+static void dispatch_argmax(ls200_context *ctx, const SitesParams &P, int traversal) {
+    if (traversal == kReference) launch_sites<false, kReference, 6, true>(ctx, P);
+    else launch_sites<false, kLadderClimb, 6, true>(ctx, P);
+}
+
 static size_t align_up(size_t n) { return (n + 255) & ~size_t(255); }
 
-}  // namespace ls200
-
-using namespace ls200;
-
-extern "C" ls200_status ls200_march_sites(ls200_context *ctx, const ls200_site_tile *tiles,
-                                          int tile_count, int azimuth_count, int subpatch_size,
-                                          int traversal, int degrees, void *device_out,
-                                          double *seconds) {
-    return guard([&] {
+void march_sites_run(ls200_context *ctx, const ls200_site_tile *tiles, int tile_count,
+                     int azimuth_count, int subpatch_size, int traversal, bool degrees,
+                     float *device_out, double *seconds, float4 *checkpoints,
+                     uint8_t *checkpoint_flags) {
+    {
         LS_REQUIRE(ctx && tiles && device_out, "NULL argument");
         LS_REQUIRE(tile_count > 0, "tile_count must be positive");
         LS_REQUIRE(traversal == kReference || traversal == kLadderClimb,
@@ -284,8 +312,11 @@ extern "C" ls200_status ls200_march_sites(ls200_context *ctx, const ls200_site_t
         P.job_count = P.jobs_per_tile * tile_count;
         P.next_job = reinterpret_cast<unsigned long long *>(scratch + off_job);
         P.counters = ctx->counters.as<unsigned long long>();
+        P.checkpoints = checkpoints;
+        P.checkpoint_flags = checkpoint_flags;
         reset_counters(ctx);
-        if (ctx->counting) dispatch<true, 8>(ctx, P, traversal);
+        if (checkpoints) dispatch_argmax(ctx, P, traversal);
+        else if (ctx->counting) dispatch<true, 8>(ctx, P, traversal);
         else if (ctx->batch_min_blocks == 6) dispatch<false, 6>(ctx, P, traversal);
         else dispatch<false, 8>(ctx, P, traversal);
         if (seconds) LS_CUDA(cudaEventRecord(ctx->events[2], ctx->stream));
@@ -299,6 +330,21 @@ extern "C" ls200_status ls200_march_sites(ls200_context *ctx, const ls200_site_t
             seconds[1] = ms / 1000.0;
         }
         resolve_counters(ctx);
+    }
+}
+
+}  // namespace ls200
+
+using namespace ls200;
+
+extern "C" ls200_status ls200_march_sites(ls200_context *ctx, const ls200_site_tile *tiles,
+                                          int tile_count, int azimuth_count, int subpatch_size,
+                                          int traversal, int degrees, void *device_out,
+                                          double *seconds) {
+    return guard([&] {
+        march_sites_run(ctx, tiles, tile_count, azimuth_count, subpatch_size, traversal,
+                        degrees != 0, static_cast<float *>(device_out), seconds, nullptr,
+                        nullptr);
     });
 }
 

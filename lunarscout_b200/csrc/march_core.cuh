@@ -427,15 +427,37 @@ __device__ __forceinline__ MarchState begin_pass(const DemView &dem, const RaySe
 // Traversals of march_step: the reference's, and the skip ladder.
 enum Traversal { kReference = 0, kLadderClimb = 1 };
 
+// Which level-0 sample set the running maximum: nothing (NoArgmax, the
+// production kernels) or its position, distance and slope (Argmax, the
+// checkpoint of the DEM adjoint; `pass` is set by the caller).
+struct NoArgmax {
+    __device__ __forceinline__ void record(float, float, float, float, bool) {}
+};
+struct Argmax {
+    float px = 0.0f, py = 0.0f, true_m = 0.0f, slope = -1e30f;
+    int near = 0, pass = -1;
+    int current_pass = 0;
+    __device__ __forceinline__ void record(float x, float y, float distance, float value,
+                                           bool is_near) {
+        px = x;
+        py = y;
+        true_m = distance;
+        slope = value;
+        near = is_near ? 1 : 0;
+        pass = current_pass;
+    }
+};
+
 // One outer iteration of hierarchy_maximum (cuda_backend.py:672-867): one ray
 // position, the level descent (and with the ladder the climb) and the advance.
 // Returns false, leaving `st` untouched, when the pass is over (past s_end,
 // outside the DEM, or the cell left the level grid).
-template <bool kCount, int kLadder, class Table>
-__device__ __forceinline__ bool march_step(const Table &table, const DemView &dem,
-                                           const RaySegment &g, int pass_index,
-                                           float observer_z, MarchState &st, unsigned &visits,
-                                           unsigned &samples, unsigned &steps) {
+template <bool kCount, int kLadder, class Table, class Tracker>
+__device__ __forceinline__ bool march_step_tracked(const Table &table, const DemView &dem,
+                                                   const RaySegment &g, int pass_index,
+                                                   float observer_z, MarchState &st,
+                                                   unsigned &visits, unsigned &samples,
+                                                   unsigned &steps, Tracker &tracker) {
     const float radius = dem.radius;
     const float resolution = dem.resolution;
     const float observer_radius = __fadd_rn(radius, observer_z);
@@ -528,7 +550,10 @@ __device__ __forceinline__ bool march_step(const Table &table, const DemView &de
                 if (height > -20000.0f) {
                     slope = near ? __fdiv_rn(__fsub_rn(height, observer_z), true_m)
                                  : sample_slope(true_m, height, radius, observer_radius);
-                    if (slope > current) current = slope;
+                    if (slope > current) {
+                        current = slope;
+                        tracker.record(px, py, true_m, slope, near);
+                    }
                 }
                 const float magnitude = hypot_fused(dx, dy);
                 const float pixel_step = magnitude > 1e-6f ? __frcp_rn(magnitude) : 0.0005f;
@@ -568,15 +593,36 @@ __device__ __forceinline__ bool march_step(const Table &table, const DemView &de
 // ray over one DEM, starting from `current` (-1e30 for none).  Table gives
 // side(l), fallback(l), out_step(l) and cells(l).
 template <bool kCount, int kLadder, class Table>
+__device__ __forceinline__ bool march_step(const Table &table, const DemView &dem,
+                                           const RaySegment &g, int pass_index,
+                                           float observer_z, MarchState &st, unsigned &visits,
+                                           unsigned &samples, unsigned &steps) {
+    NoArgmax none;
+    return march_step_tracked<kCount, kLadder>(table, dem, g, pass_index, observer_z, st,
+                                               visits, samples, steps, none);
+}
+
+template <bool kCount, int kLadder, class Table, class Tracker>
+__device__ __forceinline__ float march_dem_tracked(const Table &table, const DemView &dem,
+                                                   const RaySegment &g, int pass_index,
+                                                   float observer_z, float current,
+                                                   unsigned &visits, unsigned &samples,
+                                                   unsigned &steps, Tracker &tracker) {
+    MarchState st = begin_pass(dem, g, current);
+    while (march_step_tracked<kCount, kLadder>(table, dem, g, pass_index, observer_z, st,
+                                               visits, samples, steps, tracker)) {
+    }
+    return st.current;
+}
+
+template <bool kCount, int kLadder, class Table>
 __device__ __forceinline__ float march_dem(const Table &table, const DemView &dem,
                                            const RaySegment &g, int pass_index,
                                            float observer_z, float current, unsigned &visits,
                                            unsigned &samples, unsigned &steps) {
-    MarchState st = begin_pass(dem, g, current);
-    while (march_step<kCount, kLadder>(table, dem, g, pass_index, observer_z, st, visits,
-                                       samples, steps)) {
-    }
-    return st.current;
+    NoArgmax none;
+    return march_dem_tracked<kCount, kLadder>(table, dem, g, pass_index, observer_z, current,
+                                              visits, samples, steps, none);
 }
 
 }  // namespace ls200

@@ -67,6 +67,26 @@ class _SiteTileStruct(ctypes.Structure):
                 ("observer_elevation_m", ctypes.c_float)]
 
 
+def site_tile_structs(tiles):
+    """ls200_site_tile array for ``tiles`` (SiteTile) and the handle arrays it
+    points into (keep both alive for the call)."""
+    tiles = list(tiles)
+    if not tiles:
+        raise ValueError("at least one tile is required")
+    handle_arrays = []
+    structs = (_SiteTileStruct * len(tiles))()
+    for slot, tile in zip(structs, tiles):
+        handles = (ctypes.c_void_p * len(tile.dems))(*[d.handle.value for d in tile.dems])
+        handle_arrays.append(handles)
+        slot.dems = ctypes.cast(handles, ctypes.c_void_p)
+        slot.dem_count = len(tile.dems)
+        slot.tile_column = int(tile.tile_column)
+        slot.tile_row = int(tile.tile_row)
+        slot.maximum_distance_m = float(tile.maximum_distance_m)
+        slot.observer_elevation_m = float(tile.observer_elevation_m)
+    return structs, handle_arrays
+
+
 class DeviceDem:
     """A DEM (level 0 + max pyramid + georeference) resident on the device."""
 
@@ -354,22 +374,9 @@ class CudaSession:
         per tile).  Returns (segment + setup seconds, march seconds)."""
         if traversal not in TRAVERSALS:
             raise ValueError(f"traversal must be one of {sorted(TRAVERSALS)}")
-        tiles = list(tiles)
-        if not tiles:
-            raise ValueError("at least one tile is required")
-        handle_arrays = []
-        structs = (_SiteTileStruct * len(tiles))()
-        for slot, tile in zip(structs, tiles):
-            handles = (ctypes.c_void_p * len(tile.dems))(*[d.handle.value for d in tile.dems])
-            handle_arrays.append(handles)
-            slot.dems = ctypes.cast(handles, ctypes.c_void_p)
-            slot.dem_count = len(tile.dems)
-            slot.tile_column = int(tile.tile_column)
-            slot.tile_row = int(tile.tile_row)
-            slot.maximum_distance_m = float(tile.maximum_distance_m)
-            slot.observer_elevation_m = float(tile.observer_elevation_m)
+        structs, _keep = site_tile_structs(tiles)
         seconds = np.zeros(2, dtype=np.float64)
-        call("ls200_march_sites", self._ctx, ctypes.cast(structs, ctypes.c_void_p), len(tiles),
+        call("ls200_march_sites", self._ctx, ctypes.cast(structs, ctypes.c_void_p), len(structs),
              int(azimuth_count),
              int(subpatch_size), TRAVERSALS[traversal], 1 if degrees else 0,
              ctypes.c_void_p(device_out), seconds.ctypes.data)

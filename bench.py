@@ -506,6 +506,86 @@ def multisite_accuracy(session, grids, regional, tiles, chosen, out, batched):
     return summary
 
 
+ADJOINT_FD_CELLS = 200
+
+
+def adjoint_benchmark(session, args, rank):
+    """The differentiable-lighting configuration: a 256 x 256 study area (4
+    tiles) in the middle of a 2048 x 2048 DEM at 10 m (fBm + craters), 1440
+    azimuths, 20 km rays, loss = weighted (uniform [0, 1], seeded) mean smooth
+    sun fraction over 29.53 days at 2 h steps (355 times).  Times the forward
+    (march with argmax checkpoints, sun directions, loss) and the adjoint, and
+    checks central finite differences at +-0.05 m on 200 cells."""
+    import torch
+
+    from lunarscout_b200.adjoint import SunLossProblem
+    from lunarscout_b200.synthetic import SyntheticDemSpec, sun_vectors, synthetic_dem
+
+    dem = synthetic_dem(SyntheticDemSpec(2048, 10.0, craters=300, crater_max_m=4000.0, seed=31))
+    tiles = [(896, 896), (1024, 896), (896, 1024), (1024, 1024)]
+    rng = np.random.default_rng(32 + rank)
+    weights = rng.uniform(0.0, 1.0, size=(len(tiles), TILE, TILE)).astype(np.float32)
+    vectors = sun_vectors(np.arange(355, dtype=np.float64) * 2.0)
+    problem = SunLossProblem(session, [dem], tiles, weights, vectors,
+                             maximum_distance_m=20_000.0, observer_elevation_m=OBSERVER_M,
+                             azimuth_count=AZIMUTHS, traversal="ladder")
+    heights = torch.from_numpy(dem.elevation_m).cuda()
+    problem.forward_value([heights])
+    problem.backward_value(1.0)
+    forward, backward, walls = [], [], []
+    for _ in range(3):
+        started = time.perf_counter()
+        loss = problem.forward_value()
+        problem.backward_value(1.0)
+        walls.append(time.perf_counter() - started)
+        forward.append(problem.last_seconds["forward_march"]
+                       + problem.last_seconds["forward_lighting"])
+        backward.append(problem.last_seconds["backward"])
+    forward_s, backward_s = statistics.median(forward), statistics.median(backward)
+    result = {
+        "metric": "DEM adjoint / forward time (smooth sun fraction, 20 km, 1440 az)",
+        "loss": loss, "forward_ms": 1000.0 * forward_s, "backward_ms": 1000.0 * backward_s,
+        "adjoint_over_forward": backward_s / forward_s,
+        "forward_plus_adjoint_over_forward": (forward_s + backward_s) / forward_s,
+        "wall_ms_forward_and_backward": 1000.0 * statistics.median(walls),
+        "rays": len(tiles) * TILE * TILE * AZIMUTHS, "time_steps": len(vectors),
+        "disk_radius_deg": problem.disk_radius_deg,
+        "model": "smooth disk fraction (differentiable model, not the reference's 16-slice "
+                 "fraction)",
+    }
+    if not args.skip_cpu:
+        problem.forward_value([heights])
+        problem.replay_value()
+        (grad,) = problem.backward_value(1.0)
+        grad = grad.cpu().numpy()
+        magnitude = np.abs(grad).ravel()
+        live = np.flatnonzero(magnitude > 1e-3 * magnitude.max())
+        cells = rng.choice(live, min(ADJOINT_FD_CELLS, live.size), replace=False)
+        observer = np.zeros(grad.shape, dtype=bool)
+        observer[896:1152, 896:1152] = True
+        errors = {"terrain": [], "observer": []}
+        for index in cells:
+            y, x = divmod(int(index), dem.width)
+            h = heights.clone()
+            h[y, x] += 0.05
+            plus = problem.replay_value([h])
+            h[y, x] -= 0.1
+            minus = problem.replay_value([h])
+            error = abs((plus - minus) / 0.1 - grad[y, x]) / abs(grad[y, x])
+            errors["observer" if observer[y, x] else "terrain"].append(error)
+        problem.set_heights([heights])
+        summary = {}
+        for kind, values in errors.items():
+            if values:
+                v = np.array(values)
+                summary[kind] = {"cells": int(v.size), "median_rel": float(np.median(v)),
+                                 "p90_rel": float(np.quantile(v, 0.9)),
+                                 "within_1e-3": float(np.mean(v <= 1e-3))}
+        result["finite_differences_0.05m_fixed_sampling"] = summary
+    problem.close()
+    return result
+
+
 def run_ours(args):
     import torch
     import torch.distributed as dist
@@ -635,6 +715,7 @@ def run_ours(args):
     del segments
     multisite = None if args.skip_multisite else multisite_benchmark(session, stream, args,
                                                                      world, rank)
+    adjoint = None if args.skip_adjoint else adjoint_benchmark(session, args, rank)
 
     fp32_peak = session.fp32_probe()
     pass_times = np.array(pass_times)
@@ -683,6 +764,7 @@ def run_ours(args):
             "segment_generation_ms_per_tile": segment_seconds * 1000.0,
             "lightmap": lighting,
             "multisite": multisite,
+            "adjoint": adjoint,
         }
         print(json.dumps(line), flush=True)
     session.close()
@@ -786,6 +868,8 @@ def main():
     parser.add_argument("--skip-cpu", action="store_true")
     parser.add_argument("--skip-multisite", action="store_true",
                         help="leave out the uneven multi-site batched-vs-plain leg")
+    parser.add_argument("--skip-adjoint", action="store_true",
+                        help="leave out the DEM-adjoint (differentiable lighting) leg")
     parser.add_argument("--profile", nargs="?", const="site", choices=("site", "multisite"),
                         help="small profiling case, no timing: 'site' = one site-scale tile "
                              "(two march steps, two lighting launches); 'multisite' = four "

@@ -281,6 +281,11 @@ ls200_status ls200_sun_loss_forward(ls200_context *ctx, const ls200_site_tile *t
 ls200_status ls200_sun_loss_backward(ls200_context *ctx, double grad_output,
                                      double *const *device_grads, int grad_count,
                                      double *seconds);
+/* The last forward's loss re-evaluated at the DEMs' current heights with its
+ * sampling held fixed: every ray's horizon is recomputed (FP64) from its
+ * recorded winning sample.  A following backward differentiates this
+ * function, whose finite differences then match the adjoint. */
+ls200_status ls200_sun_loss_replay(ls200_context *ctx, double *loss);
 /* Host copies of the last forward's checkpoints (rays x 4 float: px, py,
  * distance m, slope; flags = pass << 1 | near, 0xff for none), sun
  * directions ([tiles, T, 16384] x (azimuth, elevation) degrees) and horizons

@@ -104,6 +104,16 @@ class SunLossProblem:
         self.last_seconds["forward_lighting"] = float(seconds[1])
         return float(loss.value)
 
+    def replay_value(self, heights=None) -> float:
+        """The last forward's loss at the given heights with its sampling (the
+        march's culling, step positions and winning samples) held fixed; a
+        following backward differentiates this function."""
+        if heights is not None:
+            self.set_heights(heights)
+        loss = ctypes.c_double()
+        call("ls200_sun_loss_replay", self.session.context, ctypes.byref(loss))
+        return float(loss.value)
+
     def backward_value(self, grad_output: float = 1.0):
         """float64 gradients of grad_output x the last forward's loss."""
         import torch

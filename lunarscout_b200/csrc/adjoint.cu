@@ -35,7 +35,9 @@ struct AdjointState {
     DeviceBuffer patches;       // [tiles, 128, 128] heights for the lighting frames
     DeviceBuffer weights;       // [tiles, 16384]
     DeviceBuffer gradient;      // [tiles, 16384, A] double: dL/dh
+    DeviceBuffer replayed;      // [tiles, 16384, A] double horizons of the last replay
     DeviceBuffer loss;          // 1 double
+    bool use_replayed = false;  // the backward differentiates the last replay
     std::vector<ls200_dem *> dems;  // the shared DEM stack, primary first
     std::vector<int2> origins;      // tile origins (column, row)
     std::vector<float> observer;    // observer elevation per tile
@@ -73,7 +75,8 @@ struct HorizonAt {
     bool left_live, right_live;
 };
 
-__device__ __forceinline__ HorizonAt horizon_at(const float *__restrict__ row, int azimuth_count,
+template <class T>
+__device__ __forceinline__ HorizonAt horizon_at(const T *__restrict__ row, int azimuth_count,
                                                 float azimuth_deg) {
     HorizonAt h;
     const double position = static_cast<double>(azimuth_deg) * (azimuth_count / 360.0);
@@ -102,6 +105,7 @@ __device__ __forceinline__ double disk_fraction_slope(double u) {
 
 struct LossParams {
     const float *horizons;
+    const double *replayed;  // used instead of `horizons` when not NULL
     const float2 *directions;
     const float *weights;
     double *gradient;  // backward only
@@ -119,14 +123,15 @@ __global__ void __launch_bounds__(128) loss_kernel(const __grid_constant__ LossP
         pixel / kPatch < P.valid[tile].y) {
         const float w = P.weights[static_cast<size_t>(tile) * kPatch * kPatch + pixel];
         if (w != 0.0f) {
-            const float *row =
-                P.horizons + (static_cast<size_t>(tile) * kPatch * kPatch + pixel) * P.azimuth_count;
+            const size_t base =
+                (static_cast<size_t>(tile) * kPatch * kPatch + pixel) * P.azimuth_count;
             const float2 *dir = P.directions + static_cast<size_t>(tile) * P.time_count * kPatch *
                                                    kPatch + pixel;
             double sum = 0.0;
             for (int t = 0; t < P.time_count; ++t) {
                 const float2 d = dir[static_cast<size_t>(t) * kPatch * kPatch];
-                const HorizonAt h = horizon_at(row, P.azimuth_count, d.x);
+                const HorizonAt h = P.replayed ? horizon_at(P.replayed + base, P.azimuth_count, d.x)
+                                               : horizon_at(P.horizons + base, P.azimuth_count, d.x);
                 sum += disk_fraction((static_cast<double>(d.y) - h.value) / P.radius_deg);
             }
             value = static_cast<double>(w) * sum / P.time_count;
@@ -152,13 +157,13 @@ __global__ void __launch_bounds__(128) horizon_gradient_kernel(const __grid_cons
     if (pixel % kPatch >= P.valid[tile].x || pixel / kPatch >= P.valid[tile].y) return;
     const float w = P.weights[static_cast<size_t>(tile) * kPatch * kPatch + pixel];
     if (w == 0.0f) return;
-    const float *row = P.horizons + base;
     const float2 *dir =
         P.directions + static_cast<size_t>(tile) * P.time_count * kPatch * kPatch + pixel;
     const double factor = static_cast<double>(w) * P.scale / P.radius_deg;
     for (int t = 0; t < P.time_count; ++t) {
         const float2 d = dir[static_cast<size_t>(t) * kPatch * kPatch];
-        const HorizonAt h = horizon_at(row, P.azimuth_count, d.x);
+        const HorizonAt h = P.replayed ? horizon_at(P.replayed + base, P.azimuth_count, d.x)
+                                       : horizon_at(P.horizons + base, P.azimuth_count, d.x);
         const double u = (static_cast<double>(d.y) - h.value) / P.radius_deg;
         const double g = -factor * disk_fraction_slope(u);  // dL/dh at the interpolated h
         if (g == 0.0) continue;
@@ -214,56 +219,118 @@ struct ScatterParams {
     long long rays_per_tile, total_rays;
 };
 
-__global__ void __launch_bounds__(128) scatter_kernel(const __grid_constant__ ScatterParams P) {
-    const long long ray = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (ray >= P.total_rays) return;
-    const double g = P.gradient[ray];
-    const uint8_t flag = P.flags[ray];
-    if (g == 0.0 || flag == 0xff) return;
+// The winning sample of one ray, re-evaluated in FP64 at the DEMs' current
+// heights: its slope and the slope's partials with respect to the sample's
+// terrain height and the observer's (the reference's near-field and
+// spherical slope formulas, nh/cuda_backend.py:812-830), with the bilinear
+// corners of both heights.
+struct SampleTerms {
+    double slope, d_height, d_observer;
+    Corners height_corners, observer_corners;
+    int pass;
+};
+
+__device__ __forceinline__ SampleTerms sample_terms(const ScatterParams &P, long long ray,
+                                                    uint8_t flag) {
+    SampleTerms s;
     const int tile = static_cast<int>(ray / P.rays_per_tile);
     const int pixel = static_cast<int>((ray - tile * P.rays_per_tile) / P.azimuth_count);
     const float4 c = P.checkpoints[ray];
-    const int pass = flag >> 1;
+    s.pass = flag >> 1;
     const bool near = flag & 1;
-    const double slope = c.w;
-    const double g_slope = g * (180.0 / M_PI) / (1.0 + slope * slope);
-    const ScatterDem &dem = P.dems[pass];
+    const ScatterDem &dem = P.dems[s.pass];
     const ScatterDem &primary = P.dems[0];
-    // Winning sample height and the observer's terrain height.
-    const Corners hc = bilinear_corners(dem.width, dem.height, c.x, c.y);
+    s.height_corners = bilinear_corners(dem.width, dem.height, c.x, c.y);
     double height = 0.0;
-    for (int k = 0; k < 4; ++k) height += hc.weight[k] * dem.level0[hc.index[k]];
+    for (int k = 0; k < 4; ++k)
+        height += s.height_corners.weight[k] * dem.level0[s.height_corners.index[k]];
     const int column = P.origins[tile].x + pixel % kPatch;
     const int row = P.origins[tile].y + pixel / kPatch;
-    const Corners oc = bilinear_corners(primary.width, primary.height, static_cast<float>(column),
-                                        static_cast<float>(row));
+    s.observer_corners = bilinear_corners(primary.width, primary.height,
+                                          static_cast<float>(column), static_cast<float>(row));
     double observer_z = P.observer[tile];
-    for (int k = 0; k < 4; ++k) observer_z += oc.weight[k] * primary.level0[oc.index[k]];
+    for (int k = 0; k < 4; ++k)
+        observer_z += s.observer_corners.weight[k] * primary.level0[s.observer_corners.index[k]];
     const double distance = c.z;
-    double d_height, d_observer;
     if (near) {
-        d_height = 1.0 / distance;
-        d_observer = -1.0 / distance;
+        s.slope = (height - observer_z) / distance;
+        s.d_height = 1.0 / distance;
+        s.d_observer = -1.0 / distance;
     } else {
         const double radius = dem.radius;
         const double rho = radius + observer_z;
         const double point = radius + height;
         const double z = (point * point - rho * rho - distance * distance) / (2.0 * rho);
         const double lx2 = distance * distance - z * z;
-        const double dslope_dz = lx2 > 0.0 ? distance * distance / (lx2 * sqrt(lx2)) : 1e6;
-        d_height = dslope_dz * point / rho;
-        d_observer = dslope_dz * (-1.0 - z / rho);
+        const double x = lx2 > 0.0 ? sqrt(lx2) : 1e-6;
+        const double dslope_dz = lx2 > 0.0 ? distance * distance / (lx2 * x) : 1e6;
+        s.slope = z / x;
+        s.d_height = dslope_dz * point / rho;
+        s.d_observer = dslope_dz * (-1.0 - z / rho);
     }
+    return s;
+}
+
+__global__ void __launch_bounds__(128) scatter_kernel(const __grid_constant__ ScatterParams P) {
+    const long long ray = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (ray >= P.total_rays) return;
+    const double g = P.gradient[ray];
+    const uint8_t flag = P.flags[ray];
+    if (g == 0.0 || flag == 0xff) return;
+    const SampleTerms s = sample_terms(P, ray, flag);
+    const double g_slope = g * (180.0 / M_PI) / (1.0 + s.slope * s.slope);
+    const ScatterDem &dem = P.dems[s.pass];
+    const ScatterDem &primary = P.dems[0];
     for (int k = 0; k < 4; ++k) {
-        if (hc.weight[k] != 0.0) atomicAdd(dem.grad + hc.index[k], g_slope * d_height * hc.weight[k]);
-        if (oc.weight[k] != 0.0)
-            atomicAdd(primary.grad + oc.index[k], g_slope * d_observer * oc.weight[k]);
+        if (s.height_corners.weight[k] != 0.0)
+            atomicAdd(dem.grad + s.height_corners.index[k],
+                      g_slope * s.d_height * s.height_corners.weight[k]);
+        if (s.observer_corners.weight[k] != 0.0)
+            atomicAdd(primary.grad + s.observer_corners.index[k],
+                      g_slope * s.d_observer * s.observer_corners.weight[k]);
     }
+}
+
+// Horizons (degrees, FP64) of every ray from its recorded winning sample at
+// the DEMs' current heights: the march's discrete choices held fixed.
+__global__ void __launch_bounds__(128) replay_kernel(const __grid_constant__ ScatterParams P,
+                                                    double *__restrict__ horizons) {
+    const long long ray = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (ray >= P.total_rays) return;
+    const uint8_t flag = P.flags[ray];
+    if (flag == 0xff) {
+        horizons[ray] = -INFINITY;
+        return;
+    }
+    const SampleTerms s = sample_terms(P, ray, flag);
+    horizons[ray] = atan(s.slope) * (180.0 / M_PI);
+}
+
+static ScatterParams scatter_params(AdjointState &st, double *const *device_grads) {
+    ScatterParams S{};
+    S.checkpoints = st.checkpoints.as<float4>();
+    S.flags = st.flags.as<uint8_t>();
+    S.gradient = st.gradient.as<double>();
+    for (size_t d = 0; d < st.dems.size(); ++d) {
+        const ls200_dem *dem = st.dems[d];
+        S.dems[d] = ScatterDem{dem->level0, device_grads ? device_grads[d] : nullptr, dem->width,
+                               dem->height,
+                               static_cast<double>(static_cast<float>(dem->projection[0]))};
+    }
+    for (int t = 0; t < st.tile_count; ++t) {
+        S.origins[t] = st.origins[t];
+        S.observer[t] = st.observer[t];
+    }
+    S.azimuth_count = st.azimuth_count;
+    S.rays_per_tile = static_cast<long long>(kPatch) * kPatch * st.azimuth_count;
+    S.total_rays = S.rays_per_tile * st.tile_count;
+    return S;
 }
 
 static LossParams loss_params(AdjointState &st) {
     LossParams P{};
     P.horizons = st.horizons.as<float>();
+    P.replayed = st.use_replayed ? st.replayed.as<double>() : nullptr;
     P.directions = st.directions.as<float2>();
     P.weights = st.weights.as<float>();
     P.gradient = st.gradient.as<double>();
@@ -363,6 +430,7 @@ extern "C" ls200_status ls200_sun_loss_forward(ls200_context *ctx, const ls200_s
         B.time_count = sun->count;
         directions_launch(ctx, B, tile_count, st.directions.as<float2>());
         LS_CUDA(cudaMemsetAsync(st.loss.ptr, 0, sizeof(double), ctx->stream));
+        st.use_replayed = false;
         LossParams P = loss_params(st);
         loss_kernel<<<dim3(plane / 128, tile_count), 128, 0, ctx->stream>>>(P);
         LS_CUDA(cudaGetLastError());
@@ -401,22 +469,7 @@ extern "C" ls200_status ls200_sun_loss_backward(ls200_context *ctx, double grad_
         const size_t plane = static_cast<size_t>(kPatch) * kPatch;
         horizon_gradient_kernel<<<dim3(plane / 128, st.tile_count), 128, 0, ctx->stream>>>(P);
         LS_CUDA(cudaGetLastError());
-        ScatterParams S{};
-        S.checkpoints = st.checkpoints.as<float4>();
-        S.flags = st.flags.as<uint8_t>();
-        S.gradient = st.gradient.as<double>();
-        for (int d = 0; d < grad_count; ++d) {
-            const ls200_dem *dem = st.dems[d];
-            S.dems[d] = ScatterDem{dem->level0, device_grads[d], dem->width, dem->height,
-                                   static_cast<double>(static_cast<float>(dem->projection[0]))};
-        }
-        for (int t = 0; t < st.tile_count; ++t) {
-            S.origins[t] = st.origins[t];
-            S.observer[t] = st.observer[t];
-        }
-        S.azimuth_count = st.azimuth_count;
-        S.rays_per_tile = static_cast<long long>(plane) * st.azimuth_count;
-        S.total_rays = S.rays_per_tile * st.tile_count;
+        const ScatterParams S = scatter_params(st, device_grads);
         const unsigned blocks = static_cast<unsigned>((S.total_rays + 127) / 128);
         scatter_kernel<<<blocks, 128, 0, ctx->stream>>>(S);
         LS_CUDA(cudaGetLastError());
@@ -427,6 +480,30 @@ extern "C" ls200_status ls200_sun_loss_backward(ls200_context *ctx, double grad_
             LS_CUDA(cudaEventElapsedTime(&ms, ctx->events[0], ctx->events[1]));
             *seconds = ms / 1000.0;
         }
+    });
+}
+
+extern "C" ls200_status ls200_sun_loss_replay(ls200_context *ctx, double *loss) {
+    return guard([&] {
+        LS_REQUIRE(ctx && loss, "NULL argument");
+        std::lock_guard<std::mutex> hold(ctx->lock);
+        LS_REQUIRE(ctx->adjoint && ctx->adjoint->ready, "no forward pass to replay");
+        AdjointState &st = *ctx->adjoint;
+        activate(ctx);
+        const ScatterParams S = scatter_params(st, nullptr);
+        st.replayed.reserve(sizeof(double) * static_cast<size_t>(S.total_rays));
+        replay_kernel<<<static_cast<unsigned>((S.total_rays + 127) / 128), 128, 0, ctx->stream>>>(
+            S, st.replayed.as<double>());
+        LS_CUDA(cudaGetLastError());
+        st.use_replayed = true;
+        LS_CUDA(cudaMemsetAsync(st.loss.ptr, 0, sizeof(double), ctx->stream));
+        const LossParams P = loss_params(st);
+        const size_t plane = static_cast<size_t>(kPatch) * kPatch;
+        loss_kernel<<<dim3(plane / 128, st.tile_count), 128, 0, ctx->stream>>>(P);
+        LS_CUDA(cudaGetLastError());
+        LS_CUDA(cudaMemcpyAsync(loss, st.loss.ptr, sizeof(double), cudaMemcpyDeviceToHost,
+                                ctx->stream));
+        LS_CUDA(cudaStreamSynchronize(ctx->stream));
     });
 }
 

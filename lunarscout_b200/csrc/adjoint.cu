@@ -143,7 +143,27 @@ __global__ void __launch_bounds__(128) loss_kernel(const __grid_constant__ LossP
         value += __shfl_down_sync(0xffffffffu, value, offset);
     if ((threadIdx.x & 31) == 0) partial[threadIdx.x >> 5] = value;
     __syncthreads();
-    if (threadIdx.x == 0) atomicAdd(P.loss, partial[0] + partial[1] + partial[2] + partial[3]);
+    // One partial per block, summed in a fixed order by sum_partials_kernel,
+    // so that the loss is the same bits on every call.
+    if (threadIdx.x == 0)
+        P.loss[1 + blockIdx.y * gridDim.x + blockIdx.x] =
+            partial[0] + partial[1] + partial[2] + partial[3];
+}
+
+__global__ void sum_partials_kernel(double *loss, int count) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    double total = 0.0;
+    for (int i = 0; i < count; ++i) total += loss[1 + i];
+    loss[0] = total;
+}
+
+// loss_kernel + the ordered sum into loss[0] (loss holds 1 + blocks doubles).
+static void launch_loss(ls200_context *ctx, const LossParams &P, int tile_count) {
+    const int blocks_per_tile = kPatch * kPatch / 128;
+    loss_kernel<<<dim3(blocks_per_tile, tile_count), 128, 0, ctx->stream>>>(P);
+    LS_CUDA(cudaGetLastError());
+    sum_partials_kernel<<<1, 32, 0, ctx->stream>>>(P.loss, blocks_per_tile * tile_count);
+    LS_CUDA(cudaGetLastError());
 }
 
 // dL/dh[pixel, azimuth] (each thread owns one pixel's row; zeroes it first).
@@ -402,7 +422,7 @@ extern "C" ls200_status ls200_sun_loss_forward(ls200_context *ctx, const ls200_s
         st.directions.reserve(sizeof(float2) * tile_count * plane * sun->count);
         st.patches.reserve(sizeof(float) * tile_count * plane + sizeof(int2) * tile_count);
         st.weights.reserve(sizeof(float) * tile_count * plane);
-        st.loss.reserve(sizeof(double));
+        st.loss.reserve(sizeof(double) * (1 + tile_count * plane / 128));
         ctx->scratch.reserve(sizeof(float) * 12 * tile_count * plane);
         if (seconds) LS_CUDA(cudaEventRecord(ctx->events[0], ctx->stream));
         LS_CUDA(cudaMemcpyAsync(st.weights.ptr, device_weights, sizeof(float) * tile_count * plane,
@@ -429,11 +449,8 @@ extern "C" ls200_status ls200_sun_loss_forward(ls200_context *ctx, const ls200_s
         B.time_start = 0;
         B.time_count = sun->count;
         directions_launch(ctx, B, tile_count, st.directions.as<float2>());
-        LS_CUDA(cudaMemsetAsync(st.loss.ptr, 0, sizeof(double), ctx->stream));
         st.use_replayed = false;
-        LossParams P = loss_params(st);
-        loss_kernel<<<dim3(plane / 128, tile_count), 128, 0, ctx->stream>>>(P);
-        LS_CUDA(cudaGetLastError());
+        launch_loss(ctx, loss_params(st), tile_count);
         if (seconds) LS_CUDA(cudaEventRecord(ctx->events[1], ctx->stream));
         LS_CUDA(cudaMemcpyAsync(loss, st.loss.ptr, sizeof(double), cudaMemcpyDeviceToHost,
                                 ctx->stream));
@@ -496,11 +513,7 @@ extern "C" ls200_status ls200_sun_loss_replay(ls200_context *ctx, double *loss) 
             S, st.replayed.as<double>());
         LS_CUDA(cudaGetLastError());
         st.use_replayed = true;
-        LS_CUDA(cudaMemsetAsync(st.loss.ptr, 0, sizeof(double), ctx->stream));
-        const LossParams P = loss_params(st);
-        const size_t plane = static_cast<size_t>(kPatch) * kPatch;
-        loss_kernel<<<dim3(plane / 128, st.tile_count), 128, 0, ctx->stream>>>(P);
-        LS_CUDA(cudaGetLastError());
+        launch_loss(ctx, loss_params(st), st.tile_count);
         LS_CUDA(cudaMemcpyAsync(loss, st.loss.ptr, sizeof(double), cudaMemcpyDeviceToHost,
                                 ctx->stream));
         LS_CUDA(cudaStreamSynchronize(ctx->stream));

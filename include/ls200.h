@@ -249,6 +249,24 @@ ls200_status ls200_lighting_device_noalloc(ls200_context *ctx, int tile_count,
                                            const float *horizons, const float *device_vectors,
                                            int vector_count, int time_start, int time_count,
                                            int signal, void *out);
+/* ---- mission duration: src/lunarscout/_numba_horizon/mission_duration.py:
+ *      164-256 (reduce_longest_candidate_duration_stream) over the condition
+ *      of mission_duration_pipeline.py:88-349 (fraction >= threshold, and
+ *      with Earth vectors Earth margin >= threshold), fused with the
+ *      lightmap so the condition stream is never materialised ----
+ * Tiles as in ls200_lighting_device (device patch DEMs and horizons, host
+ * geotransforms / projections / windows); sun (and optional earth) vector
+ * tables of the same length T; sample_hours (host f64[T]) the duration
+ * credited to each sample; start_windows (host int32[I][2]) the (first, end)
+ * sample indices of each candidate start window, I <= 64.  out (device)
+ * float32 [tiles, I, 16384]: the longest right-censored run per window, in
+ * hours or, with output_days, days. */
+ls200_status ls200_mission_duration_device(
+    ls200_context *ctx, int tile_count, const float *patch_dems, const double *geo_transforms,
+    const double *projections, const int32_t *windows, const float *horizons,
+    const ls200_vectors *sun, const ls200_vectors *earth, float sun_threshold,
+    float earth_threshold, const double *sample_hours, const int32_t *start_windows,
+    int interval_count, int output_days, float *out);
 /* Diagnostic: sun fraction at given (azimuth, elevation) in degrees for n
  * horizon rows float32[n,1440] (lightmap.py:32-73). */
 ls200_status ls200_sun_fraction(ls200_context *ctx, const float *horizons,

@@ -258,6 +258,159 @@ void directions_launch(ls200_context *ctx, LightingBatch &B, int tiles, float2 *
     LS_CUDA(cudaGetLastError());
 }
 
+// Condition bits of the mission-duration product (nh/mission_duration_pipeline.py:
+// the per-sample condition fraction >= sun_threshold, and with Earth vectors
+// earth margin >= earth_threshold), 32 time steps per word: bits
+// [tiles, 16384, words].  Same per-sample arithmetic as lighting_kernel.
+template <bool kEarth>
+__global__ void __launch_bounds__(128) condition_kernel(const __grid_constant__ LightingBatch B,
+                                                        const float *__restrict__ earth,
+                                                        float sun_threshold,
+                                                        float earth_threshold, int words,
+                                                        int words_per_thread,
+                                                        uint32_t *__restrict__ bits) {
+    const int tile = blockIdx.z;
+    const int index = blockIdx.x * blockDim.x + threadIdx.x;
+    if (index >= kPatch * kPatch) return;
+    const TileGeo &g = B.tiles[tile];
+    const int sample = index % kPatch, line = index / kPatch;
+    const size_t plane = static_cast<size_t>(kPatch) * kPatch;
+    uint32_t *row = bits + (static_cast<size_t>(tile) * plane + index) * words;
+    const int w0 = blockIdx.y * words_per_thread;
+    const int w1 = min(w0 + words_per_thread, words);
+    if (sample >= g.valid_width || line >= g.valid_height) {
+        for (int w = w0; w < w1; ++w) row[w] = 0u;
+        return;
+    }
+    Frame32 f;
+    const float *src = B.frames + (static_cast<size_t>(tile) * plane + index) * 12;
+#pragma unroll
+    for (int k = 0; k < 12; ++k) f.v[k] = src[k];
+    const float *horizon = B.horizons + (static_cast<size_t>(tile) * plane + index) * kAzimuths;
+    for (int w = w0; w < w1; ++w) {
+        uint32_t word = 0u;
+        for (int j = 0; j < 32; ++j) {
+            const int t = w * 32 + j;
+            if (t >= B.time_count) break;
+            const float *v = B.vectors + 3 * static_cast<size_t>(t);
+            float azimuth_deg, elevation;
+            body_direction(f, __ldg(v), __ldg(v + 1), __ldg(v + 2), azimuth_deg, elevation);
+            bool on = sun_fraction(horizon, azimuth_deg, elevation) >= sun_threshold;
+            if (kEarth && on) {
+                const float *e = earth + 3 * static_cast<size_t>(t);
+                body_direction(f, __ldg(e), __ldg(e + 1), __ldg(e + 2), azimuth_deg, elevation);
+                on = horizon_margin(horizon, azimuth_deg, elevation) >= earth_threshold;
+            }
+            word |= static_cast<uint32_t>(on) << j;
+        }
+        row[w] = word;
+    }
+}
+
+// Longest right-censored candidate run per start interval
+// (nh/mission_duration.py:212-256), one thread per pixel over the bits.  For
+// a run of true samples [rs, re] and a start window [ws, we) the candidate
+// starts at max(rs, ws) when that lies in the window and accrues every
+// sample's duration through re; the answer per interval is the maximum over
+// runs.  Durations are summed in sample order in FP64 as the reference does
+// (or read from exact prefix sums when every sample duration is an integer).
+constexpr int kMaxDurationIntervals = 64;
+
+struct DurationParams {
+    const uint32_t *bits;
+    const double *hours;   // [T] sample durations
+    const double *prefix;  // [T + 1] exact prefix sums, or NULL
+    const int2 *windows;   // [I] (first, end) sample indices of each start window
+    float *out;            // [tiles, I, 16384]
+    int words, time_count, interval_count, tiles, days;
+    int2 valid[kMaxBatchTiles];
+};
+
+__device__ __forceinline__ double run_hours(const DurationParams &P, int first, int last) {
+    if (P.prefix) return P.prefix[last + 1] - P.prefix[first];
+    double sum = 0.0;
+    for (int t = first; t <= last; ++t) sum += P.hours[t];
+    return sum;
+}
+
+__global__ void __launch_bounds__(128) duration_kernel(const __grid_constant__ DurationParams P) {
+    const int tile = blockIdx.y;
+    const int index = blockIdx.x * blockDim.x + threadIdx.x;
+    if (index >= kPatch * kPatch) return;
+    const size_t plane = static_cast<size_t>(kPatch) * kPatch;
+    double longest[kMaxDurationIntervals];
+    for (int i = 0; i < P.interval_count; ++i) longest[i] = 0.0;
+    const bool valid =
+        index % kPatch < P.valid[tile].x && index / kPatch < P.valid[tile].y;
+    if (valid) {
+        const uint32_t *row = P.bits + (static_cast<size_t>(tile) * plane + index) * P.words;
+        int run_start = -1;
+        for (int t = 0; t <= P.time_count; ++t) {
+            const bool on = t < P.time_count && ((row[t >> 5] >> (t & 31)) & 1u);
+            if (on) {
+                if (run_start < 0) run_start = t;
+                continue;
+            }
+            if (run_start < 0) continue;
+            const int run_end = t - 1;
+            for (int i = 0; i < P.interval_count; ++i) {
+                const int2 w = P.windows[i];
+                const int first = max(run_start, w.x);
+                if (first >= w.y || first > run_end) continue;
+                const double d = run_hours(P, first, run_end);
+                if (d > longest[i]) longest[i] = d;
+            }
+            run_start = -1;
+        }
+    }
+    for (int i = 0; i < P.interval_count; ++i) {
+        const double v = P.days ? longest[i] / 24.0 : longest[i];
+        P.out[(static_cast<size_t>(tile) * P.interval_count + i) * plane + index] =
+            static_cast<float>(v);
+    }
+}
+
+void mission_duration_launch(ls200_context *ctx, LightingBatch &B, int tiles,
+                             const float *earth, float sun_threshold, float earth_threshold,
+                             uint32_t *bits, const double *hours, const double *prefix,
+                             const int2 *windows, int interval_count, bool days, float *out) {
+    LS_REQUIRE(tiles >= 1 && tiles <= kMaxBatchTiles, "1 to 32 tiles per launch");
+    LS_REQUIRE(interval_count >= 1 && interval_count <= kMaxDurationIntervals,
+               "1 to 64 start intervals");
+    ensure_lighting_constants(ctx);
+    dim3 grid_frames(kPatch * kPatch / 128, tiles);
+    frames_kernel<<<grid_frames, 128, 0, ctx->stream>>>(B);
+    LS_CUDA(cudaGetLastError());
+    const int words = (B.time_count + 31) / 32;
+    const int chunk_steps = lighting_chunk(ctx, tiles, B.time_count);
+    const int words_per_thread = std::max(1, chunk_steps / 32);
+    dim3 grid(kPatch * kPatch / 128, (words + words_per_thread - 1) / words_per_thread, tiles);
+    if (earth)
+        condition_kernel<true><<<grid, 128, 0, ctx->stream>>>(B, earth, sun_threshold,
+                                                             earth_threshold, words,
+                                                             words_per_thread, bits);
+    else
+        condition_kernel<false><<<grid, 128, 0, ctx->stream>>>(B, nullptr, sun_threshold,
+                                                              earth_threshold, words,
+                                                              words_per_thread, bits);
+    LS_CUDA(cudaGetLastError());
+    DurationParams P{};
+    P.bits = bits;
+    P.hours = hours;
+    P.prefix = prefix;
+    P.windows = windows;
+    P.out = out;
+    P.words = words;
+    P.time_count = B.time_count;
+    P.interval_count = interval_count;
+    P.tiles = tiles;
+    P.days = days ? 1 : 0;
+    for (int t = 0; t < tiles; ++t)
+        P.valid[t] = make_int2(B.tiles[t].valid_width, B.tiles[t].valid_height);
+    duration_kernel<<<dim3(kPatch * kPatch / 128, tiles), 128, 0, ctx->stream>>>(P);
+    LS_CUDA(cudaGetLastError());
+}
+
 void sun_fraction_launch(ls200_context *ctx, const float *horizons, const float *azimuth_deg,
                          const float *elevation_deg, int n, float *out) {
     ensure_lighting_constants(ctx);

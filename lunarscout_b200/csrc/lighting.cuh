@@ -48,6 +48,17 @@ void ensure_lighting_constants(ls200_context *ctx);
 // elevation deg) at every pixel and time step of [time_start, +time_count):
 // out [tiles, time_count, 16384] (zero outside the valid rectangle).
 void directions_launch(ls200_context *ctx, LightingBatch &batch, int tiles, float2 *out);
+// The mission-duration product fused with the lighting: per-pixel condition
+// bits (sun fraction >= sun_threshold [and, with `earth`, Earth margin >=
+// earth_threshold]) into `bits` ([tiles, 16384, ceil(T/32)] words), then the
+// longest right-censored run per start interval into out [tiles, I, 16384]
+// (hours, or days).  hours: device [T] sample durations; prefix: device
+// [T + 1] exact prefix sums or NULL; windows: device [I] (first, end) sample
+// indices of each start window.
+void mission_duration_launch(ls200_context *ctx, LightingBatch &batch, int tiles,
+                             const float *earth, float sun_threshold, float earth_threshold,
+                             uint32_t *bits, const double *hours, const double *prefix,
+                             const int2 *windows, int interval_count, bool days, float *out);
 
 #ifdef LS200_LIGHTING_KERNELS
 // Slice half-heights and their normaliser (set by ensure_lighting_constants).

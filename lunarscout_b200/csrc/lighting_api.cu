@@ -1,10 +1,14 @@
 // C-ABI entry points of the lighting products.
 #include "lighting.cuh"
 
+#include <cmath>
+#include <vector>
+
 namespace ls200 {
 
 struct LightingState {
     DeviceBuffer dem, horizons, frames, out;
+    DeviceBuffer duration_frames, duration_bits, duration_tables;  // mission duration
     TileGeo geo{};
     bool loaded = false;
     std::set<ls200_vectors *> vectors;  // live vector tables of the context
@@ -193,6 +197,93 @@ ls200_status ls200_lighting_device(ls200_context *ctx, int tile_count, const flo
         B.time_start = signal == kSignalPsr ? 0 : time_start;
         B.time_count = signal == kSignalPsr ? vectors->count : time_count;
         lighting_launch(ctx, B, tile_count, signal);
+    });
+}
+
+ls200_status ls200_mission_duration_device(
+    ls200_context *ctx, int tile_count, const float *patch_dems, const double *geo_transforms,
+    const double *projections, const int32_t *windows, const float *horizons,
+    const ls200_vectors *sun, const ls200_vectors *earth, float sun_threshold,
+    float earth_threshold, const double *sample_hours, const int32_t *start_windows,
+    int interval_count, int output_days, float *out) {
+    return guard([&] {
+        LS_REQUIRE(ctx && patch_dems && geo_transforms && projections && windows && horizons &&
+                       sun && sample_hours && start_windows && out,
+                   "NULL argument");
+        LS_REQUIRE(tile_count >= 1 && tile_count <= kMaxBatchTiles,
+                   "tile_count must be between 1 and 32");
+        LS_REQUIRE(interval_count >= 1 && interval_count <= 64,
+                   "interval_count must be between 1 and 64");
+        LS_REQUIRE(sun->ctx == ctx && sun->count > 0, "sun vectors belong to another context");
+        LS_REQUIRE(!earth || (earth->ctx == ctx && earth->count == sun->count),
+                   "earth vectors must match the sun vectors' time axis");
+        const int count = sun->count;
+        std::vector<int2> intervals(interval_count);
+        for (int i = 0; i < interval_count; ++i) {
+            intervals[i] = make_int2(start_windows[2 * i], start_windows[2 * i + 1]);
+            LS_REQUIRE(intervals[i].x >= 0 && intervals[i].x <= intervals[i].y &&
+                           intervals[i].y <= count,
+                       "start windows must be sample index ranges within the time axis");
+        }
+        bool integral = true;
+        double total = 0.0;
+        for (int t = 0; t < count; ++t) {
+            LS_REQUIRE(std::isfinite(sample_hours[t]) && sample_hours[t] >= 0.0,
+                       "sample durations must be finite and non-negative");
+            integral = integral && sample_hours[t] == std::floor(sample_hours[t]);
+            total += sample_hours[t];
+        }
+        integral = integral && total < 9.0e15;
+        std::vector<double> prefix;
+        if (integral) {
+            prefix.resize(count + 1);
+            prefix[0] = 0.0;
+            for (int t = 0; t < count; ++t) prefix[t + 1] = prefix[t] + sample_hours[t];
+        }
+        std::lock_guard<std::mutex> hold(ctx->lock);
+        activate(ctx);
+        LightingState &st = state_of(ctx);
+        LightingBatch B{};
+        for (int t = 0; t < tile_count; ++t) {
+            std::memcpy(B.tiles[t].gt, geo_transforms + 6 * t, sizeof B.tiles[t].gt);
+            std::memcpy(B.tiles[t].proj, projections + 6 * t, sizeof B.tiles[t].proj);
+            B.tiles[t].tile_x = windows[4 * t + 0];
+            B.tiles[t].tile_y = windows[4 * t + 1];
+            B.tiles[t].valid_width = windows[4 * t + 2];
+            B.tiles[t].valid_height = windows[4 * t + 3];
+            check_valid(B.tiles[t].valid_width, B.tiles[t].valid_height);
+        }
+        const size_t plane = static_cast<size_t>(kPatch) * kPatch;
+        const size_t words = (static_cast<size_t>(count) + 31) / 32;
+        const size_t frames_bytes = sizeof(float) * 12 * tile_count * plane;
+        const size_t bits_bytes = sizeof(uint32_t) * tile_count * plane * words;
+        const size_t table_bytes = sizeof(double) * (2 * size_t(count) + 1) +
+                                   sizeof(int2) * interval_count;
+        st.duration_frames.reserve(frames_bytes);
+        st.duration_bits.reserve(bits_bytes);
+        st.duration_tables.reserve(table_bytes);
+        double *d_hours = st.duration_tables.as<double>();
+        double *d_prefix = d_hours + count;
+        int2 *d_windows = reinterpret_cast<int2 *>(d_prefix + count + 1);
+        LS_CUDA(cudaMemcpyAsync(d_hours, sample_hours, sizeof(double) * count,
+                                cudaMemcpyHostToDevice, ctx->stream));
+        if (integral)
+            LS_CUDA(cudaMemcpyAsync(d_prefix, prefix.data(), sizeof(double) * (count + 1),
+                                    cudaMemcpyHostToDevice, ctx->stream));
+        LS_CUDA(cudaMemcpyAsync(d_windows, intervals.data(), sizeof(int2) * interval_count,
+                                cudaMemcpyHostToDevice, ctx->stream));
+        B.patch_dem = patch_dems;
+        B.horizons = horizons;
+        B.vectors = sun->data;
+        B.frames = st.duration_frames.as<float>();
+        B.time_start = 0;
+        B.time_count = count;
+        mission_duration_launch(ctx, B, tile_count, earth ? earth->data : nullptr,
+                                sun_threshold, earth_threshold, st.duration_bits.as<uint32_t>(),
+                                d_hours, integral ? d_prefix : nullptr, d_windows,
+                                interval_count, output_days != 0, out);
+        // The host tables above must outlive their copies.
+        LS_CUDA(cudaStreamSynchronize(ctx->stream));
     });
 }
 

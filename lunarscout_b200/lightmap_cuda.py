@@ -174,6 +174,60 @@ class LightmapCudaSession:
             for tile in batch:
                 yield np.ascontiguousarray(tile)
 
+    def mission_durations(self, dem, horizons_deg, sun_vectors_m, *, tile_y: int, tile_x: int,
+                          valid_height: int, valid_width: int, sample_hours,
+                          start_windows, earth_vectors_m=None, sun_threshold: float = 0.5,
+                          earth_threshold: float = 0.0, days: bool = False) -> np.ndarray:
+        """Longest right-censored condition run per candidate start window,
+        float32 [I, valid_height, valid_width] (hours, or days): the condition
+        (sun fraction >= sun_threshold [and Earth margin >= earth_threshold])
+        evaluated and reduced on the device without materialising it
+        (nh/mission_duration.py:164-256).  ``sample_hours`` f64[T] is the
+        duration credited to each sample; ``start_windows`` int[I, 2] the
+        (first, end) sample indices of each candidate start window."""
+        import torch
+
+        sun = np.ascontiguousarray(validate_vectors(sun_vectors_m), dtype=np.float32)
+        earth = (None if earth_vectors_m is None else
+                 np.ascontiguousarray(validate_vectors(earth_vectors_m), dtype=np.float32))
+        if earth is not None and len(earth) != len(sun):
+            raise ValueError("Earth and Sun vectors must share the time axis")
+        hours = np.ascontiguousarray(sample_hours, dtype=np.float64)
+        if hours.shape != (len(sun),):
+            raise ValueError("sample_hours must have one entry per time step")
+        windows = np.ascontiguousarray(start_windows, dtype=np.int32).reshape(-1, 2)
+        horizons = np.ascontiguousarray(horizons_deg, dtype=np.float32)
+        if horizons.shape != (PATCH_SIZE, PATCH_SIZE, AZIMUTH_COUNT):
+            raise ValueError("horizons must have shape (128, 128, 1440)")
+        if not 1 <= valid_width <= PATCH_SIZE or not 1 <= valid_height <= PATCH_SIZE:
+            raise ValueError("valid patch dimensions must be between 1 and 128")
+        patch = torch.from_numpy(
+            patch_elevations(dem, tile_y, tile_x, valid_height, valid_width)).cuda()
+        device_horizons = torch.from_numpy(horizons).cuda()
+        out = torch.empty((len(windows), PATCH_SIZE * PATCH_SIZE), dtype=torch.float32,
+                          device="cuda")
+        geo = np.ascontiguousarray(dem.geo_transform, dtype=np.float64)
+        projection = projection_array(dem.projection)
+        window = np.array([tile_x, tile_y, valid_width, valid_height], dtype=np.int32)
+        torch.cuda.synchronize()
+        with self._lock, self._context.lock:
+            sun_table = DeviceVectors(self._context.handle, sun)
+            earth_table = None if earth is None else DeviceVectors(self._context.handle, earth)
+            try:
+                call("ls200_mission_duration_device", self._context.handle, 1,
+                     ctypes.c_void_p(patch.data_ptr()), geo.ctypes.data, projection.ctypes.data,
+                     window.ctypes.data, ctypes.c_void_p(device_horizons.data_ptr()),
+                     sun_table.handle, None if earth_table is None else earth_table.handle,
+                     float(sun_threshold), float(earth_threshold), hours.ctypes.data,
+                     windows.ctypes.data, len(windows), 1 if days else 0,
+                     ctypes.c_void_p(out.data_ptr()))
+            finally:
+                sun_table.close()
+                if earth_table is not None:
+                    earth_table.close()
+        grid = out.cpu().numpy().reshape(len(windows), PATCH_SIZE, PATCH_SIZE)
+        return np.ascontiguousarray(grid[:, :valid_height, :valid_width])
+
     def sun_fraction(self, horizons: np.ndarray, azimuth_deg, elevation_deg) -> np.ndarray:
         """Diagnostic: fraction of the disk at (azimuth, elevation) above each
         horizon row (lightmap.py:32-73)."""

@@ -144,3 +144,53 @@ def test_psr_pinned_buffer_and_validation(psr_session, site):
         psr_session.compute_patch(site["dem"], buffer, site["sun"][:10], tile_y=500, tile_x=0)
     with pytest.raises(ValueError):
         psr_session.compute_patch(site["dem"], buffer[:64], site["sun"][:10], tile_y=0, tile_x=0)
+
+
+def _duration_inputs(hours, stop, bounds):
+    following = np.append(hours[1:], stop)
+    sample_hours = np.minimum(following, stop) - hours
+    accepts = np.stack([(hours >= lo) & (hours < hi) for lo, hi in bounds])
+    windows = np.array([[np.searchsorted(hours, lo, "left"), np.searchsorted(hours, hi, "left")]
+                        for lo, hi in bounds], dtype=np.int32)
+    return sample_hours, accepts, windows
+
+
+@pytest.mark.parametrize("stop", [750.0, 746.5])
+def test_mission_durations_reduce_the_device_conditions_exactly(lighting_session, site, stop):
+    hours = np.arange(len(site["sun"]), dtype=np.float64) * 6.0
+    bounds = [(0.0, 168.0), (168.0, 336.0), (336.0, 504.0), (504.0, 744.0), (100.0, 101.0)]
+    sample_hours, accepts, windows = _duration_inputs(hours, stop, bounds)
+    fractions = np.stack(list(lighting_session.iter_patch_fraction_tiles(
+        site["dem"], site["horizons"], site["sun"], **site["tile"])))
+    margins = np.stack(list(lighting_session.iter_patch_margin_tiles(
+        site["dem"], site["horizons"], site["earth"], **site["tile"])))
+    got = lighting_session.mission_durations(site["dem"], site["horizons"], site["sun"],
+                                             sample_hours=sample_hours, start_windows=windows,
+                                             **site["tile"])
+    expected = products.longest_duration(fractions >= np.float32(0.5), sample_hours, accepts)
+    np.testing.assert_array_equal(got, expected.astype(np.float32))
+    assert got.shape == (len(bounds), 40, 48) and got.max() > 0.0
+    both = lighting_session.mission_durations(
+        site["dem"], site["horizons"], site["sun"], earth_vectors_m=site["earth"], days=True,
+        sample_hours=sample_hours, start_windows=windows, **site["tile"])
+    expected = products.longest_duration(
+        (fractions >= np.float32(0.5)) & (margins >= np.float32(0.0)), sample_hours,
+        accepts) / 24.0
+    np.testing.assert_array_equal(both, expected.astype(np.float32))
+
+
+def test_mission_durations_against_the_reference_cpu_chain(lighting_session, site):
+    hours = np.arange(len(site["sun"]), dtype=np.float64) * 6.0
+    bounds = [(0.0, 240.0), (240.0, 480.0), (480.0, 744.0)]
+    sample_hours, accepts, windows = _duration_inputs(hours, 750.0, bounds)
+    got = lighting_session.mission_durations(site["dem"], site["horizons"], site["sun"],
+                                             sample_hours=sample_hours, start_windows=windows,
+                                             **site["tile"])
+    cpu = products.lighting_tiles(site["dem"], site["horizons"], site["sun"], **site["tile"])
+    expected = products.longest_duration(cpu >= np.float32(0.5), sample_hours, accepts)
+    # Fractions differ from the CPU backend by <= 1e-4 (atan2f); a condition
+    # can flip only for fractions within that of the threshold.
+    differ = got != expected.astype(np.float32)
+    near = (np.abs(cpu - np.float32(0.5)) <= 1e-4).any(axis=0)
+    assert np.all(near[differ.any(axis=0)])
+    assert differ.mean() <= 0.01

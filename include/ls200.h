@@ -249,6 +249,25 @@ ls200_status ls200_lighting_device_noalloc(ls200_context *ctx, int tile_count,
                                            const float *horizons, const float *device_vectors,
                                            int vector_count, int time_start, int time_count,
                                            int signal, void *out);
+/* ---- CUDA graphs of asynchronous device calls (no reference counterpart;
+ *      replaces the per-chunk launch-and-wait loop of
+ *      src/lunarscout/_numba_horizon/lightmap_cuda.py:226-276) ----
+ * Between ls200_capture_begin and ls200_capture_end the context's stream
+ * records instead of running: asynchronous entry points (ls200_lighting_device
+ * over its time chunks, the *_device march / segment entries) become graph
+ * nodes bound to the device buffers they were given.  ls200_graph_launch
+ * replays the whole graph with one launch on the context's stream; buffer
+ * contents may change between launches.  A call that waits for the host
+ * inside a capture fails and invalidates it (ls200_capture_end then returns
+ * an error).  The context must use a created stream (not NULL).  Destroy
+ * graphs before their context. */
+typedef struct ls200_graph ls200_graph;
+ls200_status ls200_capture_begin(ls200_context *ctx);
+ls200_status ls200_capture_end(ls200_context *ctx, ls200_graph **out);
+ls200_status ls200_graph_launch(ls200_graph *graph);
+ls200_status ls200_graph_nodes(ls200_graph *graph, int64_t *nodes);
+ls200_status ls200_graph_destroy(ls200_graph *graph);
+
 /* ---- mission duration: src/lunarscout/_numba_horizon/mission_duration.py:
  *      164-256 (reduce_longest_candidate_duration_stream) over the condition
  *      of mission_duration_pipeline.py:88-349 (fraction >= threshold, and

@@ -93,6 +93,11 @@ SIGNATURES: dict[str, list] = {
     "ls200_sun_loss_backward": [_vp, _d, _vp, _i, _vp],
     "ls200_sun_loss_checkpoints": [_vp, _vp, _vp, _vp, _vp],
     "ls200_sun_loss_replay": [_vp, _vp],
+    "ls200_capture_begin": [_vp],
+    "ls200_capture_end": [_vp, _vp],
+    "ls200_graph_launch": [_vp],
+    "ls200_graph_nodes": [_vp, _vp],
+    "ls200_graph_destroy": [_vp],
     "ls200_mission_duration_device": [_vp, _i, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _f, _f, _vp,
                                       _vp, _i, _i, _vp],
     "ls200_set_batch_config": [_vp, _i, _i],

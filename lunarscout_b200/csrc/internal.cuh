@@ -130,7 +130,7 @@ struct ls200_context {
     ls200::CodecBuffers *codec = nullptr;
     ls200::AdjointState *adjoint = nullptr;
     // Launch configuration of the persistent multi-site march.
-    int batch_lanes_per_azimuth = 32;  // pixels of one azimuth in a 32-ray job (1..32)
+    int batch_lanes_per_azimuth = 2;   // pixels of one azimuth in a 32-ray job (1..32)
     int batch_min_blocks = 8;          // resident 128-thread blocks per SM (8 or 6)
 };
 

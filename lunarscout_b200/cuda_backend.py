@@ -54,7 +54,7 @@ class BatchConfig:
     (a power of two up to 32; the job spans 32/lanes azimuths) and ``min_blocks``
     resident 128-thread blocks per SM (8 at 64 registers or 6 at 80)."""
 
-    lanes_per_azimuth: int = 32
+    lanes_per_azimuth: int = 2
     min_blocks: int = 8
 
 

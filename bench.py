@@ -451,12 +451,121 @@ def multisite_benchmark(session, stream, args, world, rank):
         "timed_batches": SITE_BATCHES - 1, "rays_timed_per_rank": timed_rays,
         "rays": "rays of pixels inside each site DEM (partial edge tiles count their valid part)",
     }
+    result["pipeline"] = multisite_pipeline(session, stream, grids, batches[1], picks[1], out,
+                                            plain, batched)
     if rank == 0 and world == 1 and not args.skip_cpu:
         result["error_vs_fp64_deg"] = multisite_accuracy(session, grids, regional, batches[1],
                                                          picks[1], out, batched)
     for dem in site_devs + [regional_dev]:
         dem.close()
     return result
+
+
+PIPELINE_CHUNK = 1024
+
+
+def multisite_pipeline(session, stream, grids, tiles, chosen, out, plain, batched):
+    """Horizons + one year of hourly sun-fraction bytes + PSR for one batch
+    of 16 site tiles.  Batched: the persistent ladder march, then the
+    lightmap as a CUDA graph of 1024-step chunks over all tiles, then PSR.
+    Plain: per tile, the per-tile march, the chunked lightmap and PSR
+    launched eagerly.  Both keep results in HBM; CUDA events."""
+    import ctypes
+
+    import torch
+
+    from lunarscout_b200 import _native, synthetic
+    from lunarscout_b200.contract import projection_array
+    from lunarscout_b200.graphs import DeviceGraph
+    from lunarscout_b200.lightmap_cuda import DeviceVectors
+
+    count = len(tiles)
+    plane = TILE * TILE
+    hours = synthetic.hours_between("2030-01-01T00", "2031-01-01T00", 1.0)
+    vectors = synthetic.sun_vectors(hours).astype(np.float32)
+    table = DeviceVectors(session.context, vectors)
+    steps = len(vectors)
+    patches = torch.zeros((count, TILE, TILE), dtype=torch.float32, device="cuda")
+    geo = np.zeros((count, 6), dtype=np.float64)
+    proj = np.zeros((count, 6), dtype=np.float64)
+    windows = np.zeros((count, 4), dtype=np.int32)
+    for i, (tile, site) in enumerate(zip(tiles, chosen)):
+        grid = grids[site]
+        vw = min(TILE, grid.width - tile.tile_column)
+        vh = min(TILE, grid.height - tile.tile_row)
+        patches[i, :vh, :vw] = torch.from_numpy(np.ascontiguousarray(
+            grid.elevation_m[tile.tile_row:tile.tile_row + vh,
+                             tile.tile_column:tile.tile_column + vw])).cuda()
+        geo[i] = grid.geo_transform
+        proj[i] = projection_array(grid.projection)
+        windows[i] = (tile.tile_column, tile.tile_row, vw, vh)
+    frames = torch.empty(count * plane * 12, dtype=torch.float32, device="cuda")
+    chunk_out = torch.empty((count, PIPELINE_CHUNK, plane), dtype=torch.uint8, device="cuda")
+    psr = torch.empty((count, plane), dtype=torch.uint8, device="cuda")
+    lib = _native.library()
+    blocks = [(start, min(PIPELINE_CHUNK, steps - start))
+              for start in range(0, steps, PIPELINE_CHUNK)]
+    torch.cuda.synchronize()
+
+    def lighting(first, n, signal, target):
+        _native.check(lib.ls200_lighting_device(
+            session.context, n, ctypes.c_void_p(patches[first].data_ptr()),
+            geo[first:].ctypes.data, proj[first:].ctypes.data, windows[first:].ctypes.data,
+            ctypes.c_void_p(out[first].data_ptr()), table.handle, 0, steps, signal,
+            ctypes.c_void_p(frames.data_ptr()), ctypes.c_void_p(target)))
+
+    def lightmap_chunks(first, n):
+        for start, length in blocks:
+            _native.check(lib.ls200_lighting_device(
+                session.context, n, ctypes.c_void_p(patches[first].data_ptr()),
+                geo[first:].ctypes.data, proj[first:].ctypes.data, windows[first:].ctypes.data,
+                ctypes.c_void_p(out[first].data_ptr()), table.handle, start, length, 1,
+                ctypes.c_void_p(frames.data_ptr()), ctypes.c_void_p(chunk_out.data_ptr())))
+
+    batched("ladder")(tiles)
+    torch.cuda.synchronize()
+    graph = DeviceGraph.capture(session.context, lambda: lightmap_chunks(0, count))
+
+    def timed(run):
+        run()
+        torch.cuda.synchronize()
+        start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        start.record(stream)
+        run()
+        end.record(stream)
+        torch.cuda.synchronize()
+        return start.elapsed_time(end) / 1000.0
+
+    def batched_pipeline():
+        batched("ladder")(tiles)
+        graph.launch()
+        lighting(0, count, 3, psr.data_ptr())
+
+    def plain_pipeline():
+        plain(tiles)
+        for i in range(count):
+            lightmap_chunks(i, 1)
+            lighting(i, 1, 3, psr[i].data_ptr())
+
+    try:
+        batched_s = timed(batched_pipeline)
+        plain_s = timed(plain_pipeline)
+        lightmap_graph_s = timed(graph.launch)
+    finally:
+        graph.close()
+        table.close()
+    rays = sum(w[2] * w[3] for w in windows) * AZIMUTHS
+    samples = sum(w[2] * w[3] for w in windows) * steps
+    return {
+        "tiles": count, "time_steps": steps, "chunk_steps": PIPELINE_CHUNK,
+        "graph_nodes_per_batch": len(blocks) * 2,
+        "batched_seconds": batched_s, "plain_seconds": plain_s,
+        "speedup_batched_vs_plain": plain_s / batched_s,
+        "batched_rays_per_s": rays / batched_s,
+        "lightmap_graph_px_steps_per_s": samples / lightmap_graph_s,
+        "work": "ladder march (degrees) + sun-fraction bytes, 1 year hourly, in 1024-step "
+                "graph-captured chunks + PSR over the same vectors",
+    }
 
 
 def multisite_accuracy(session, grids, regional, tiles, chosen, out, batched):

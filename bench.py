@@ -73,6 +73,18 @@ def profiled_traffic(name: str):
     return None
 
 
+def max_over_ranks(value: float, world: int, device: str = "cuda") -> float:
+    """The maximum of a per-rank timing over all ranks (the job's time)."""
+    if world <= 1:
+        return value
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([value], device=device, dtype=torch.float64)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def dist_env():
     rank = int(os.environ.get("RANK", "0"))
     world = int(os.environ.get("WORLD_SIZE", "1"))
@@ -303,11 +315,7 @@ def lighting_benchmark(session, dems, segments, tiles, primary, args, world, ran
         launch()
     end.record()
     torch.cuda.synchronize()
-    elapsed = start.elapsed_time(end) / 1000.0
-    if world > 1:
-        t = torch.tensor([elapsed], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        elapsed = float(t.item())
+    elapsed = max_over_ranks(start.elapsed_time(end) / 1000.0, world)
     samples = repeats * count * plane * steps
     value = world * samples / elapsed
     table.close()
@@ -420,11 +428,7 @@ def multisite_benchmark(session, stream, args, world, rank):
             run(tiles)
         end.record(stream)
         torch.cuda.synchronize()
-        elapsed = start.elapsed_time(end) / 1000.0
-        if world > 1:
-            t = torch.tensor([elapsed], device="cuda", dtype=torch.float64)
-            dist.all_reduce(t, op=dist.ReduceOp.MAX)
-            elapsed = float(t.item())
+        elapsed = max_over_ranks(start.elapsed_time(end) / 1000.0, world)
         return world * timed_rays / elapsed, elapsed
 
     tuned = tune_batch(session, batches[0][:TUNE_TILES], device_out=out.data_ptr(),
@@ -772,11 +776,8 @@ def run_ours(args):
     end_event.record(stream)
     torch.cuda.synchronize()
     clocks = sampler.stop()
-    elapsed = start_event.elapsed_time(end_event) / 1000.0
+    elapsed = max_over_ranks(start_event.elapsed_time(end_event) / 1000.0, world)
     if world > 1:
-        t = torch.tensor([elapsed], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        elapsed = float(t.item())
         dist.barrier()
     rays = world * args.steps * RAYS_PER_TILE
     value = rays / elapsed
@@ -812,11 +813,7 @@ def run_ours(args):
         e2e_session.subpatch_hierarchical_all_passes(
             host_segments[k % 2], host_pyramids, tile_column=tiles[index][1],
             tile_row=tiles[index][0], tile_width=TILE, tile_height=TILE, subpatch_size=8)
-    e2e_elapsed = time.perf_counter() - started
-    if world > 1:
-        t = torch.tensor([e2e_elapsed], device="cuda", dtype=torch.float64)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_elapsed = float(t.item())
+    e2e_elapsed = max_over_ranks(time.perf_counter() - started, world)
     e2e_value = world * e2e_steps * RAYS_PER_TILE / e2e_elapsed
     e2e_session.close()
 

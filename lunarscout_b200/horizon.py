@@ -118,6 +118,90 @@ class HorizonTileGenerator:
         return np.frombuffer(payload, dtype="<f4").reshape(PIXEL_COUNT, AZIMUTH_COUNT).copy()
 
 
+class BatchedTileGenerator:
+    """Payloads of many patches from one persistent march per batch
+    (``CudaSession.march_sites``): on the first request for a patch it
+    marches that patch and the next ``batch_tiles - 1`` pending patches
+    together, pads and encodes each on the device and keeps the payloads
+    until they are asked for.  ``traversal="exact"`` gives the per-tile
+    path's bytes; ``"ladder"`` the skip-ladder traversal (same distance from
+    the FP64 restatement, several times faster on long rays)."""
+
+    def __init__(self, dems: Sequence[DemGrid], patches, *, session, pyramids=None,
+                 batch_tiles: int = 16, traversal: str = "exact",
+                 observer_elevation_m: float = 0.0,
+                 maximum_distance_m: float = PUBLIC_MAXIMUM_DISTANCE_M,
+                 is_done: Callable | None = None) -> None:
+        import torch
+
+        from .cuda_backend import SiteTile
+        from .file_format import TileCodec
+
+        if batch_tiles < 1:
+            raise ValueError("batch_tiles must be positive")
+        self.session = session
+        if pyramids is None:
+            pyramids = [session.build_max_pyramid(dem) for dem in dems]
+        self.device_dems = [session.upload_pyramid(p) for p in pyramids]
+        self.primary = dems[0]
+        self.patches = list(patches)
+        self.position = {(p.tile_x, p.tile_y): i for i, p in enumerate(self.patches)}
+        self.batch_tiles = int(batch_tiles)
+        self.traversal = traversal
+        self.observer = float(observer_elevation_m)
+        self.distance = float(maximum_distance_m)
+        self.is_done = is_done or (lambda patch: False)
+        self.codec = TileCodec(context=session.context)
+        self._site_tile = SiteTile
+        self.degrees = torch.empty((self.batch_tiles, PIXEL_COUNT * AZIMUTH_COUNT),
+                                   dtype=torch.float32, device="cuda")
+        self.payload = torch.empty(MAX_PAYLOAD_BYTES, dtype=torch.uint8, device="cuda")
+        self.ready: dict = {}
+
+    def close(self) -> None:
+        for dem in self.device_dems:
+            dem.close()
+        self.device_dems = []
+        self.ready.clear()
+
+    def _march(self, batch, compress: bool) -> None:
+        import torch
+
+        tiles = [self._site_tile(tuple(self.device_dems), p.tile_x, p.tile_y, self.distance,
+                                 self.observer) for p in batch]
+        torch.cuda.synchronize()
+        self.session.march_sites(tiles, device_out=self.degrees.data_ptr(),
+                                 azimuth_count=AZIMUTH_COUNT, traversal=self.traversal,
+                                 degrees=True)
+        for i, patch in enumerate(batch):
+            grid = self.degrees[i].view(PATCH_SIZE, PATCH_SIZE, AZIMUTH_COUNT)
+            if patch.width < PATCH_SIZE:
+                grid[:, patch.width:] = -50.0
+            if patch.height < PATCH_SIZE:
+                grid[patch.height:] = -50.0
+            torch.cuda.synchronize()
+            if compress:
+                size = self.codec.encode_device(self.degrees[i].data_ptr(),
+                                                self.payload.data_ptr())
+                data = self.payload[:size].cpu().numpy().tobytes()
+            else:
+                data = self.degrees[i].cpu().numpy().astype("<f4", copy=False).tobytes()
+            self.ready[(patch.tile_x, patch.tile_y)] = data
+
+    def compute(self, patch, *, compress: bool = True) -> bytes:
+        key = (patch.tile_x, patch.tile_y)
+        if key not in self.ready:
+            batch = [patch]
+            for candidate in self.patches[self.position[key] + 1:]:
+                if len(batch) == self.batch_tiles:
+                    break
+                if (candidate.tile_x, candidate.tile_y) not in self.ready and \
+                        not self.is_done(candidate):
+                    batch.append(candidate)
+            self._march(batch, compress)
+        return self.ready.pop(key)
+
+
 class _HorizonProgressAdapter:
     """Private pipeline events -> public ProgressEvent / fraction callbacks
     (ls/horizon.py:43-134): prepare 0.10, patches 0.15 + 0.85 * done/total,
@@ -209,23 +293,38 @@ def run_horizon_pipeline(dems: Sequence[DemGrid], output_directory, *,
                          overwrite: bool = False, dem_paths: Sequence[Path] | None = None,
                          maximum_distance_m: float = PUBLIC_MAXIMUM_DISTANCE_M,
                          device_id: int = 0, progress_callback=None,
-                         cancellation_requested: CancellationCheck | None = None):
+                         cancellation_requested: CancellationCheck | None = None,
+                         batch_tiles: int = 0, traversal: str = "exact"):
     """Tiles of every pending patch of ``dems[0]`` into ``output_directory``
-    (the private pipeline behind the facade; raises the pipeline's own errors)."""
+    (the private pipeline behind the facade; raises the pipeline's own errors).
+    ``batch_tiles`` > 0 marches that many patches per persistent launch."""
     from .cuda_backend import CudaSession
 
     output = Path(output_directory)
     primary = dems[0]
     store = HorizonTileStore(output)
     writer_queue_capacity = 1
+    patches = enumerate_patches(primary.width, primary.height)
     session = CudaSession(device_id)
     try:
         pyramids = (_load_pyramids(session, dems, dem_paths) if dem_paths is not None
                     else None)
-        generator = HorizonTileGenerator(dems, pyramids=pyramids, session=session,
-                                         ring=writer_queue_capacity + 2)
+        if batch_tiles > 0:
+            generator = BatchedTileGenerator(
+                dems, patches, session=session, pyramids=pyramids, batch_tiles=batch_tiles,
+                traversal=traversal, observer_elevation_m=observer_height_m,
+                maximum_distance_m=maximum_distance_m,
+                is_done=lambda p: not overwrite and store.find_existing_path(
+                    p.tile_y, p.tile_x, observer_height_m) is not None)
+        else:
+            if traversal != "exact":
+                raise ValueError("the per-tile path marches the reference traversal only")
+            generator = HorizonTileGenerator(dems, pyramids=pyramids, session=session,
+                                             ring=writer_queue_capacity + 2)
         try:
             def compute(patch):
+                if batch_tiles > 0:
+                    return generator.compute(patch, compress=compress)
                 return generator.compute(patch.tile_x, patch.tile_y,
                                          observer_elevation_m=observer_height_m,
                                          compress=compress,
@@ -236,7 +335,7 @@ def run_horizon_pipeline(dems: Sequence[DemGrid], output_directory, *,
                                            payload, compress=compress)
 
             return run_bounded_pipeline(
-                enumerate_patches(primary.width, primary.height),
+                patches,
                 store=store, compute_patch=compute, write_patch=write,
                 observer_elevation_m=observer_height_m, skip_existing=not overwrite,
                 writer_queue_capacity=writer_queue_capacity,
@@ -376,13 +475,24 @@ def generate_horizons_from_grids(
     progress_callback: ProgressCallback | None = None,
     progress_event_callback: ProgressEventCallback | None = None,
     cancellation_requested: CancellationCheck | None = None,
+    batch_tiles: int = 0,
+    traversal: str = "exact",
 ) -> Path:
     """``generate_horizons`` for in-memory DEMs (no pyramid cache files);
     ``maximum_distance_m`` is the private ray range of
-    build_subpatch_segments_numba (the public path fixes 1,000 km)."""
+    build_subpatch_segments_numba (the public path fixes 1,000 km).
+    ``batch_tiles`` > 0 marches that many patches per persistent launch;
+    ``traversal="ladder"`` (batched only) uses the skip ladder instead of the
+    reference traversal (not bit-identical to the reference's tiles)."""
     if not dems or not all(isinstance(dem, DemGrid) for dem in dems):
         raise InputError("dems must be a non-empty sequence of DemGrid, primary first.",
                          code="horizon_dem_paths_invalid")
+    if isinstance(batch_tiles, bool) or not isinstance(batch_tiles, int) or batch_tiles < 0:
+        raise InputError("batch_tiles must be a non-negative integer.",
+                         code="horizon_option_invalid", details={"argument": "batch_tiles"})
+    if traversal not in ("exact", "ladder") or (traversal == "ladder" and batch_tiles == 0):
+        raise InputError("traversal must be 'exact', or 'ladder' with batch_tiles > 0.",
+                         code="horizon_option_invalid", details={"argument": "traversal"})
     if not (isinstance(maximum_distance_m, Real) and np.isfinite(maximum_distance_m)
             and maximum_distance_m > 0.0):
         raise InputError("maximum_distance_m must be finite and positive.",
@@ -397,8 +507,9 @@ def generate_horizons_from_grids(
     return _run_mapped(tuple(dems), output, adapter, observer_height_m=float(observer_height_m),
                        compress=compress, overwrite=overwrite,
                        maximum_distance_m=float(maximum_distance_m),
-                       cancellation_requested=cancellation_requested)
+                       cancellation_requested=cancellation_requested,
+                       batch_tiles=batch_tiles, traversal=traversal)
 
 
-__all__ = ["HorizonTileGenerator", "generate_horizons", "generate_horizons_from_grids",
-           "run_horizon_pipeline"]
+__all__ = ["BatchedTileGenerator", "HorizonTileGenerator", "generate_horizons",
+           "generate_horizons_from_grids", "run_horizon_pipeline"]

@@ -428,3 +428,14 @@ def test_progress_adapter_fractions_are_monotonic_and_parse_tiles(tmp_path, caps
     assert events[2].tile_y == 128 and events[2].tile_x == 256
     assert all(e.operation == "horizons" and e.backend == "cuda" for e in events)
     assert "horizons: using cuda backend" in capsys.readouterr().out
+
+
+@pytest.mark.parametrize("options", [dict(batch_tiles=-1), dict(batch_tiles=True),
+                                     dict(traversal="ladder"),
+                                     dict(batch_tiles=4, traversal="fast")])
+def test_grid_facade_rejects_bad_batch_options(tmp_path, options):
+    from lunarscout_b200.horizon import generate_horizons_from_grids
+
+    with pytest.raises(InputError) as info:
+        generate_horizons_from_grids(tmp_path / "out", [_dem()], **options)
+    assert info.value.code == "horizon_option_invalid"

@@ -233,3 +233,26 @@ def test_generate_horizons_writes_resumes_and_overwrites(tmp_path, synthetic_pai
     for path in paths:
         twin = grid_out / path.relative_to(out)
         assert twin.read_bytes() == path.read_bytes()
+
+
+@pytest.mark.parametrize("compress", [False, True])
+def test_batched_generation_writes_the_per_tile_bytes(tmp_path, synthetic_pair, compress):
+    from lunarscout_b200.file_format import HorizonTileStore
+    from lunarscout_b200.horizon import generate_horizons_from_grids
+
+    primary, _ = synthetic_pair
+    small = type(primary)(np.ascontiguousarray(primary.elevation_m[:200, :300]),
+                          primary.geo_transform, primary.projection)
+    options = dict(observer_height_m=0.5, compress=compress, maximum_distance_m=40_000.0)
+    generate_horizons_from_grids(tmp_path / "plain", [small], **options)
+    generate_horizons_from_grids(tmp_path / "batched", [small], batch_tiles=4, **options)
+    plain = sorted((tmp_path / "plain").rglob("horizon_*"))
+    assert len(plain) == 6
+    for path in plain:
+        twin = tmp_path / "batched" / path.relative_to(tmp_path / "plain")
+        assert twin.read_bytes() == path.read_bytes(), path.name
+    generate_horizons_from_grids(tmp_path / "ladder", [small], batch_tiles=4,
+                                 traversal="ladder", **options)
+    ladder = sorted((tmp_path / "ladder").rglob("horizon_*"))
+    assert [p.name for p in ladder] == [p.name for p in plain]
+    assert all(HorizonTileStore.is_complete(p) for p in ladder)

@@ -619,6 +619,50 @@ def multisite_accuracy(session, grids, regional, tiles, chosen, out, batched):
     return summary
 
 
+GENERATE_SIDE = 512
+
+
+def generate_benchmark(primary, regional, rank):
+    """End to end through the public tile generator: the central 512 x 512
+    crop of the site DEM (16 tiles) with the regional DEM, 200 km rays,
+    .cbin files written (staged, fsynced, renamed) to a RAM-backed directory.
+    Per-tile reference traversal vs batches of 16 with the skip ladder; wall
+    clock, including segment building, encoding, D2H and the file writes."""
+    import shutil
+    import tempfile
+
+    from lunarscout_b200.contract import DemGrid
+    from lunarscout_b200.horizon import generate_horizons_from_grids
+
+    offset = (primary.width - GENERATE_SIDE) // 2
+    transform = primary.geo_transform.copy()
+    transform[0] += offset * transform[1]
+    transform[3] += offset * transform[5]
+    crop = DemGrid(np.ascontiguousarray(primary.elevation_m[offset:offset + GENERATE_SIDE,
+                                                            offset:offset + GENERATE_SIDE]),
+                   transform, primary.projection)
+    tiles = (GENERATE_SIDE // TILE) ** 2
+    base = Path("/dev/shm") if Path("/dev/shm").is_dir() else None
+    result = {"tiles": tiles, "rays": tiles * RAYS_PER_TILE, "format": ".cbin",
+              "output": "RAM-backed directory" if base else "temporary directory"}
+    for name, options in (("per_tile", {}), ("batched_ladder",
+                                             {"batch_tiles": 16, "traversal": "ladder"})):
+        folder = Path(tempfile.mkdtemp(prefix=f"ls200_{rank}_", dir=base))
+        try:
+            started = time.perf_counter()
+            generate_horizons_from_grids(folder, [crop, regional], compress=True,
+                                         maximum_distance_m=RANGE_M, **options)
+            seconds = time.perf_counter() - started
+            written = sum(1 for _ in folder.rglob("horizon_*.cbin"))
+        finally:
+            shutil.rmtree(folder, ignore_errors=True)
+        result[name] = {"seconds": seconds, "tiles_written": written,
+                        "rays_per_s": tiles * RAYS_PER_TILE / seconds}
+    result["speedup_batched_vs_per_tile"] = (result["per_tile"]["seconds"]
+                                             / result["batched_ladder"]["seconds"])
+    return result
+
+
 ADJOINT_FD_CELLS = 200
 
 
@@ -822,6 +866,9 @@ def run_ours(args):
     multisite = None if args.skip_multisite else multisite_benchmark(session, stream, args,
                                                                      world, rank)
     adjoint = None if args.skip_adjoint else adjoint_benchmark(session, args, rank)
+    # The public generator runs on device 0 (as the reference's does): 1 GPU only.
+    generate = (None if args.skip_generate or world > 1
+                else generate_benchmark(primary, regional, rank))
 
     fp32_peak = session.fp32_probe()
     pass_times = np.array(pass_times)
@@ -871,6 +918,7 @@ def run_ours(args):
             "lightmap": lighting,
             "multisite": multisite,
             "adjoint": adjoint,
+            "generate_horizons": generate,
         }
         print(json.dumps(line), flush=True)
     session.close()
@@ -976,6 +1024,8 @@ def main():
                         help="leave out the uneven multi-site batched-vs-plain leg")
     parser.add_argument("--skip-adjoint", action="store_true",
                         help="leave out the DEM-adjoint (differentiable lighting) leg")
+    parser.add_argument("--skip-generate", action="store_true",
+                        help="leave out the end-to-end tile-generator leg")
     parser.add_argument("--profile", nargs="?", const="site", choices=("site", "multisite"),
                         help="small profiling case, no timing: 'site' = one site-scale tile "
                              "(two march steps, two lighting launches); 'multisite' = four "

@@ -92,6 +92,7 @@ ls200_status ls200_context_destroy(ls200_context *ctx) {
         for (ls200_dem *dem : ctx->dems) {
             if (dem->level0) cudaFree(dem->level0);
             if (dem->cells) cudaFree(dem->cells);
+            if (dem->bounds) cudaFree(dem->bounds);
             delete dem;
         }
         ctx->dems.clear();
@@ -193,6 +194,7 @@ ls200_status ls200_dem_create(ls200_context *ctx, const float *level0, int width
             LS_CUDA(cudaMalloc(&dem->level0, sizeof(float) * cells0));
             // One allocation: sanitized level 0 followed by the packed mips.
             LS_CUDA(cudaMalloc(&dem->cells, sizeof(float) * (cells0 + size_t(dem->mip_count))));
+            LS_CUDA(cudaMalloc(&dem->bounds, sizeof(float) * (cells0 + size_t(dem->mip_count))));
             dem->mips = dem->cells + cells0;
             LS_CUDA(cudaMemcpyAsync(dem->level0, level0, sizeof(float) * cells0,
                                     cudaMemcpyHostToDevice, ctx->stream));
@@ -203,11 +205,13 @@ ls200_status ls200_dem_create(ls200_context *ctx, const float *level0, int width
                 build_pyramid_device(ctx, dem);
             }
             sanitize_level0(ctx, dem);
+            build_cell_bounds(ctx, dem);
             LS_CUDA(cudaStreamSynchronize(ctx->stream));
             ctx->dems.insert(dem);
         } catch (...) {
             if (dem->level0) cudaFree(dem->level0);
             if (dem->cells) cudaFree(dem->cells);
+            if (dem->bounds) cudaFree(dem->bounds);
             delete dem;
             throw;
         }
@@ -224,6 +228,7 @@ ls200_status ls200_dem_destroy(ls200_dem *dem) {
         dem->ctx->dems.erase(dem);
         if (dem->level0) cudaFree(dem->level0);
         if (dem->cells) cudaFree(dem->cells);
+        if (dem->bounds) cudaFree(dem->bounds);
         delete dem;
     });
 }
@@ -265,6 +270,7 @@ ls200_status ls200_dem_set_heights_device(ls200_dem *dem, const float *device_he
                                 cudaMemcpyDeviceToDevice, ctx->stream));
         build_pyramid_device(ctx, dem);
         sanitize_level0(ctx, dem);
+        build_cell_bounds(ctx, dem);
         LS_CUDA(cudaStreamSynchronize(ctx->stream));
     });
 }

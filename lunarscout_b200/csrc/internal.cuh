@@ -106,6 +106,11 @@ struct ls200_dem {
     // (NaN, +-inf, <= -20000) replaced by -32000, then the packed mips.
     float *cells = nullptr;
     float *mips = nullptr;    // = cells + height*width
+    // device, the layout of `cells`: each cell's four-cell bound, the maximum
+    // of the cell and its right, lower and lower-right neighbours on its level
+    // (-32000 for a neighbour outside the level).  The march reads one value
+    // per node visit instead of four.
+    float *bounds = nullptr;
     double geo_transform[6];
     double projection[6];
     float map_parameters[11];
@@ -156,6 +161,8 @@ int pyramid_layout(int width, int height, PyramidLevel *levels, int capacity,
 void build_pyramid_device(ls200_context *ctx, ls200_dem *dem);
 // Write the sanitized level 0 at the start of dem->cells.
 void sanitize_level0(ls200_context *ctx, ls200_dem *dem);
+// Write dem->bounds from dem->cells (after both parts of cells are final).
+void build_cell_bounds(ls200_context *ctx, ls200_dem *dem);
 
 // Segment generation into device memory.
 void segments_device(ls200_context *ctx, ls200_dem *const *dems, int dem_count,

@@ -18,7 +18,8 @@ struct MarchParams {
     const float *primary_cells;
     int primary_width, primary_height;
     float primary_m6, primary_m9;
-    const float *cells;  // sanitized level 0 + mips of the active DEM
+    const float *cells;   // sanitized level 0 + mips of the active DEM
+    const float *bounds;  // four-cell bounds of those cells
     int width, height;
     int level_count;
     int4 levels[kMaxLevels];  // (cell offset, width, height, -)
@@ -77,7 +78,7 @@ __global__ void __launch_bounds__(128, 8) march_pass_kernel(const __grid_constan
         const float initial = *out;
         current = isinf(initial) ? -1e30f : initial;
     }
-    const DemView dem{P.cells, P.width, P.height, P.level_count, resolution, column_res,
+    const DemView dem{P.cells, P.bounds, P.width, P.height, P.level_count, resolution, column_res,
                       P.radius};
     unsigned visits = 0, samples = 0, steps = 0;
     current = march_dem<kCount, kReference>(SharedLevels{table}, dem, g, P.pass_index, observer_z,
@@ -104,6 +105,7 @@ void march_pass_device(ls200_context *ctx, const MarchTile &tile, const ls200_de
     P.primary_m6 = primary->map_parameters[6];
     P.primary_m9 = primary->map_parameters[9];
     P.cells = active->cells;
+    P.bounds = active->bounds;
     P.width = active->width;
     P.height = active->height;
     P.level_count = active->level_count;

@@ -34,6 +34,7 @@ constexpr int kTilePixels = kTileSide * kTileSide;
 // device so that its float32 products round exactly as in the per-tile path.
 struct BatchDemSource {
     const float *cells;
+    const float *bounds;
     int width, height, level_count;
     int4 levels[kMaxLevels];
     float m6, m7, m9, m10, radius;
@@ -84,7 +85,7 @@ __global__ void batch_dem_kernel(const BatchDemSource *__restrict__ sources,
     BatchDem &d = dems[blockIdx.x];
     const float resolution = mean_resolution(s.m6, s.m7, s.m9, s.m10);
     if (threadIdx.x == 0)
-        d.view = DemView{s.cells, s.width, s.height, s.level_count, resolution,
+        d.view = DemView{s.cells, s.bounds, s.width, s.height, s.level_count, resolution,
                          hypot_fused(s.m6, s.m9), s.radius};
     if (threadIdx.x < s.level_count)
         fill_level(d.table, threadIdx.x, resolution, s.levels[threadIdx.x]);
@@ -269,6 +270,7 @@ void march_sites_run(ls200_context *ctx, const ls200_site_tile *tiles, int tile_
             const ls200_dem *dem = unique[i];
             BatchDemSource &s = sources[i];
             s.cells = dem->cells;
+            s.bounds = dem->bounds;
             s.width = dem->width;
             s.height = dem->height;
             s.level_count = dem->level_count;

@@ -46,7 +46,8 @@ struct LevelTable {
 
 // Everything the march of one DEM pass needs about the DEM.
 struct DemView {
-    const float *cells;  // sanitized level 0 + packed mips
+    const float *cells;   // sanitized level 0 + packed mips
+    const float *bounds;  // four-cell bound of every cell, the layout of cells
     int width, height, level_count;
     float resolution;    // mean pixel size of the DEM (m)
     float column_res;    // hypot of the column axis of the geotransform
@@ -234,6 +235,12 @@ __device__ __forceinline__ float four_cell_bound(const float *__restrict__ cells
     return fmaxf(fmaxf(v00, v10), fmaxf(v01, v11));
 }
 
+// The same value read from the precomputed bound table (one load per visit).
+__device__ __forceinline__ float cell_bound(const float *__restrict__ bounds, int4 L, int cx,
+                                            int cy) {
+    return __ldg(bounds + L.x + cy * L.y + cx);
+}
+
 // Advance (km) to the exit of the cell (cx, cy) of side 4^level pixels along
 // the tangent, + 1e-4 km, or `fallback` when the exit is not ahead
 // (cuda_backend.py:733-762).  Of max(t1, t2) only the far edge can win:
@@ -275,7 +282,7 @@ __device__ __forceinline__ float cell_exit_advance(int shift, int cx, int cy, fl
 // advance; ladder_advance climbs from `level`, returns the advance and sets
 // `reached` to the largest culled level (`level` if none).
 template <class Table>
-__device__ __forceinline__ bool ladder_culled(const Table &table, const float *__restrict__ cells,
+__device__ __forceinline__ bool ladder_culled(const Table &table, const float *__restrict__ bounds,
                                               int m, int ipx, int ipy, float px, float py,
                                               float inv_x, float inv_y, bool near, float true_m,
                                               float radius, float observer_z,
@@ -283,7 +290,7 @@ __device__ __forceinline__ bool ladder_culled(const Table &table, const float *_
                                               float current, float &step) {
     const int shift = 2 * m;
     const int cx = ipx >> shift, cy = ipy >> shift;
-    const float maximum_height = four_cell_bound(cells, table.cells(m), cx, cy);
+    const float maximum_height = cell_bound(bounds, table.cells(m), cx, cy);
     step = cell_exit_advance(shift, cx, cy, px, py, inv_x, inv_y, table.fallback(m));
     if (maximum_height < -20000.0f) return true;
     const float dh = __fsub_rn(maximum_height, observer_z);
@@ -323,7 +330,7 @@ __device__ __forceinline__ bool ladder_culled(const Table &table, const float *_
 }
 
 template <bool kCount, class Table>
-__device__ __forceinline__ float ladder_advance(const Table &table, const float *__restrict__ cells,
+__device__ __forceinline__ float ladder_advance(const Table &table, const float *__restrict__ bounds,
                                                 int level, int top, int ipx, int ipy, float px,
                                                 float py, float inv_x, float inv_y, bool near,
                                                 float true_m, float radius, float observer_z,
@@ -336,7 +343,7 @@ __device__ __forceinline__ float ladder_advance(const Table &table, const float 
     for (int m = level + 1; m <= top; ++m) {
         float step;
         if (kCount) ++visits;
-        if (!ladder_culled(table, cells, m, ipx, ipy, px, py, inv_x, inv_y, near, true_m, radius,
+        if (!ladder_culled(table, bounds, m, ipx, ipy, px, py, inv_x, inv_y, near, true_m, radius,
                            observer_z, observer_radius, inverse_denominator, current, step))
             break;
         best = step;
@@ -417,11 +424,17 @@ struct MarchState {
     float s;            // path position (km)
     float current;      // maximum slope so far (-1e30 for none)
     int level_hint;     // level of the previous step
+    // side(level_hint + 1) (NaN at the top level) and side(level_hint)
+    // (-inf at level 0): the level search keeps level_hint whenever
+    // !(side_up <= footprint) && side_here <= footprint.
+    float side_up, side_here;
 };
 
+// side_here = +inf sends the first step through the full level search.
 __device__ __forceinline__ MarchState begin_pass(const DemView &dem, const RaySegment &g,
                                                  float current) {
-    return MarchState{g.s_start > 0.001f ? g.s_start : 0.001f, current, dem.level_count - 1};
+    return MarchState{g.s_start > 0.001f ? g.s_start : 0.001f, current, dem.level_count - 1,
+                      __int_as_float(0x7fffffff), INFINITY};
 }
 
 // Traversals of march_step: the reference's, and the skip ladder.
@@ -471,6 +484,7 @@ __device__ __forceinline__ bool march_step_tracked(const Table &table, const Dem
     float s = st.s;
     float current = st.current;
     int level_hint = st.level_hint;
+    float side_up = st.side_up, side_here = st.side_here;
     if (!(s <= g.s_end)) return false;
     {
         if (kCount) ++steps;
@@ -498,10 +512,16 @@ __device__ __forceinline__ bool march_step_tracked(const Table &table, const Dem
         // whose side fits the footprint (or 0).  Sides grow with the level,
         // so that level is also found by moving up or down from the previous
         // step's level, which usually takes one comparison.
+        // The two sides around the previous level sit in registers, so the
+        // usual step decides with two comparisons and no table read.
         int level = level_hint;
-        while (level < top_level && table.side(level + 1) <= footprint) ++level;
-        while (level > 0 && !(table.side(level) <= footprint)) --level;
-        level_hint = level;
+        if (side_up <= footprint || !(side_here <= footprint)) {
+            while (level < top_level && table.side(level + 1) <= footprint) ++level;
+            while (level > 0 && !(table.side(level) <= footprint)) --level;
+            level_hint = level;
+            side_up = level < top_level ? table.side(level + 1) : __int_as_float(0x7fffffff);
+            side_here = level > 0 ? table.side(level) : -INFINITY;
+        }
         // The tangent and its reciprocals depend only on delta.
         const float dx = quartic_tangent(g.a1, g.a2, g.a3, g.a4, delta);
         const float dy = quartic_tangent(g.b1, g.b2, g.b3, g.b4, delta);
@@ -519,7 +539,7 @@ __device__ __forceinline__ bool march_step_tracked(const Table &table, const Dem
                 ray_out = true;
                 break;
             }
-            const float maximum_height = four_cell_bound(cells, L, cx, cy);
+            const float maximum_height = cell_bound(dem.bounds, L, cx, cy);
             const float skip =
                 cell_exit_advance(shift, cx, cy, px, py, inv_x, inv_y, table.fallback(level));
             bool culled = maximum_height < -20000.0f;
@@ -534,7 +554,7 @@ __device__ __forceinline__ bool march_step_tracked(const Table &table, const Dem
                 float advance = skip;
                 if (kLadder != kReference) {
                     int reached;
-                    advance = ladder_advance<kCount>(table, cells, level, top_level, ipx, ipy,
+                    advance = ladder_advance<kCount>(table, dem.bounds, level, top_level, ipx, ipy,
                                                      px, py, inv_x, inv_y, near, true_m, radius,
                                                      observer_z, observer_radius,
                                                      inverse_denominator, current, skip, visits,
@@ -586,6 +606,8 @@ __device__ __forceinline__ bool march_step_tracked(const Table &table, const Dem
     st.s = s;
     st.current = current;
     st.level_hint = level_hint;
+    st.side_up = side_up;
+    st.side_here = side_here;
     return true;
 }
 

@@ -3,7 +3,7 @@
 // (finite and > -20000) of its 4x4 block of the level below, or -32000 when
 // the block has no valid cell.  One launch per level, all on the context
 // stream with no host round trip between levels.
-#include "internal.cuh"
+#include "march_core.cuh"
 
 namespace ls200 {
 
@@ -57,6 +57,44 @@ void sanitize_level0(ls200_context *ctx, ls200_dem *dem) {
     const int blocks = static_cast<int>(std::min<long long>((n + 255) / 256,
                                                             ctx->props.multiProcessorCount * 8));
     sanitize_kernel<<<blocks, 256, 0, ctx->stream>>>(dem->level0, n, dem->cells);
+    LS_CUDA(cudaGetLastError());
+}
+
+struct BoundLevels {
+    int4 level[kMaxLevels];  // (cell offset, width, height, -), as the march's tables
+    int count;
+};
+
+// bounds[i] = four_cell_bound of cell i, through the march's own function so
+// that the stored value is the one the march would compute.  Grid-stride over
+// every cell of every level.
+__global__ void cell_bounds_kernel(const float *__restrict__ cells, float *__restrict__ bounds,
+                                   const __grid_constant__ BoundLevels T, long long total) {
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
+         i += (long long)gridDim.x * blockDim.x) {
+        for (int l = 0; l < T.count; ++l) {
+            const int4 L = T.level[l];
+            const long long local = i - L.x;
+            if (local < 0 || local >= static_cast<long long>(L.y) * L.z) continue;
+            const int cy = static_cast<int>(local / L.y);
+            const int cx = static_cast<int>(local - static_cast<long long>(cy) * L.y);
+            bounds[i] = four_cell_bound(cells, L, cx, cy);
+            break;
+        }
+    }
+}
+
+void build_cell_bounds(ls200_context *ctx, ls200_dem *dem) {
+    BoundLevels T{};
+    const int cells0 = dem->width * dem->height;
+    T.count = dem->level_count;
+    for (int l = 0; l < dem->level_count; ++l)
+        T.level[l] = make_int4(l == 0 ? 0 : cells0 + dem->levels[l].offset,
+                               dem->levels[l].width, dem->levels[l].height, 0);
+    const long long total = static_cast<long long>(cells0) + dem->mip_count;
+    const int blocks = static_cast<int>(std::min<long long>(
+        (total + 255) / 256, static_cast<long long>(ctx->props.multiProcessorCount) * 8));
+    cell_bounds_kernel<<<blocks, 256, 0, ctx->stream>>>(dem->cells, dem->bounds, T, total);
     LS_CUDA(cudaGetLastError());
 }
 

@@ -255,6 +255,59 @@ LIGHT_TILES = 8
 LIGHT_FLOPS_PER_SAMPLE = 150
 
 
+def safe_haven_benchmark(session, lib, count, patches, geo, proj, windows, horizons, world):
+    """The fused safe-haven product (Sun fraction and Earth margin per pixel
+    and step, then the per-month run reducer) over two years of hourly Sun
+    and Earth vectors (17,545 steps, 25 month bands) on the same tiles."""
+    import ctypes
+    from datetime import datetime, timedelta, timezone
+
+    import torch
+
+    from lunarscout_b200 import _native, synthetic
+    from lunarscout_b200.lightmap_cuda import DeviceVectors
+    from lunarscout_b200.safe_haven import month_bands, month_indices
+
+    hours = synthetic.hours_between("2030-01-01T00", "2032-01-01T00", 1.0)
+    start = datetime(2030, 1, 1, tzinfo=timezone.utc)
+    times = [start + timedelta(hours=float(h)) for h in hours]
+    bands = month_bands(times)
+    months = month_indices(times, bands)
+    sun = DeviceVectors(session.context, synthetic.sun_vectors(hours).astype(np.float32))
+    earth = DeviceVectors(session.context, synthetic.earth_vectors(hours).astype(np.float32))
+    out = torch.empty((count, len(bands), TILE * TILE), dtype=torch.float32, device="cuda")
+
+    def launch():
+        _native.check(lib.ls200_safe_haven_device(
+            session.context, count, ctypes.c_void_p(patches.data_ptr()), geo.ctypes.data,
+            proj.ctypes.data, windows.ctypes.data, ctypes.c_void_p(horizons.data_ptr()),
+            sun.handle, earth.handle, ctypes.c_float(0.2), ctypes.c_float(2.0),
+            ctypes.c_float(1.0), months.ctypes.data, len(bands),
+            ctypes.c_void_p(out.data_ptr())))
+
+    launch()
+    torch.cuda.synchronize()
+    repeats = 3
+    begin, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    begin.record()
+    for _ in range(repeats):
+        launch()
+    end.record()
+    torch.cuda.synchronize()
+    elapsed = max_over_ranks(begin.elapsed_time(end) / 1000.0, world)
+    sun.close()
+    earth.close()
+    px_steps = repeats * count * TILE * TILE * len(hours)
+    finite = torch.isfinite(out)
+    return {
+        "metric": "safe-haven px·steps/s (Sun fraction + Earth margin + monthly run reducer)",
+        "value": world * px_steps / elapsed, "unit": "px·steps/s", "tiles_per_launch": count,
+        "time_steps": len(hours), "month_bands": len(bands), "launches": repeats,
+        "ms_per_tile_two_years": 1000.0 * elapsed / (repeats * count),
+        "defined_fraction": float(finite.float().mean()),
+    }
+
+
 def lighting_benchmark(session, dems, segments, tiles, primary, args, world, rank):
     """Sun-fraction bytes for one year of hourly steps on the timed tiles'
     horizons, computed from the device-resident march output (horizon ->
@@ -319,7 +372,10 @@ def lighting_benchmark(session, dems, segments, tiles, primary, args, world, ran
     samples = repeats * count * plane * steps
     value = world * samples / elapsed
     table.close()
+    haven = safe_haven_benchmark(session, lib, count, patches, geo, proj, windows, horizons,
+                                 world)
     result = {
+        "safe_haven": haven,
         "metric": "lightmap px·steps/s (sun-fraction bytes, 1 year hourly)",
         "value": value, "unit": "px·steps/s", "tiles_per_launch": count,
         "time_steps": steps, "launches": repeats,

@@ -286,6 +286,25 @@ ls200_status ls200_mission_duration_device(
     const ls200_vectors *sun, const ls200_vectors *earth, float sun_threshold,
     float earth_threshold, const double *sample_hours, const int32_t *start_windows,
     int interval_count, int output_days, float *out);
+
+/* ---- safe haven: src/lunarscout/_numba_horizon/safe_haven.py:75-243
+ *      (reduce_safe_haven_patch_stream) over the fraction and Earth-margin
+ *      streams that safe_haven_pipeline.py:240-272 feeds it, fused with the
+ *      lightmap so neither stream is materialised ----
+ * Tiles as in ls200_lighting_device; sun and earth vector tables of the same
+ * length T; month_index_of (host int32[T]) the month band of each time step
+ * (-1 for none, else < band_count).  Low Sun is fraction < sunlight_threshold
+ * (in [0, 1]); an Earth outage is margin < earth_threshold_deg (finite).
+ * out (device) float32 [tiles, band_count, 16384]: per band the longest
+ * low-Sun run that overlapped an outage within the band, times
+ * time_step_hours (> 0); NaN where the band saw no outage or only outages,
+ * and outside each tile's valid rectangle. */
+ls200_status ls200_safe_haven_device(
+    ls200_context *ctx, int tile_count, const float *patch_dems, const double *geo_transforms,
+    const double *projections, const int32_t *windows, const float *horizons,
+    const ls200_vectors *sun, const ls200_vectors *earth, float sunlight_threshold,
+    float earth_threshold_deg, float time_step_hours, const int32_t *month_index_of,
+    int band_count, float *out);
 /* Diagnostic: sun fraction at given (azimuth, elevation) in degrees for n
  * horizon rows float32[n,1440] (lightmap.py:32-73). */
 ls200_status ls200_sun_fraction(ls200_context *ctx, const float *horizons,

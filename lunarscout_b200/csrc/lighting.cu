@@ -411,6 +411,192 @@ void mission_duration_launch(ls200_context *ctx, LightingBatch &B, int tiles,
     LS_CUDA(cudaGetLastError());
 }
 
+// Condition bits of the safe-haven product (safe_haven.py:156-160): per pixel
+// and time step, low Sun (sun fraction < sunlight_threshold) and Earth outage
+// (Earth margin < earth_threshold, degrees).  Word-major [tiles, words, 16384]:
+// a warp's 32 pixels write, and the reducer reads, 128 contiguous bytes.
+// Same per-sample arithmetic as lighting_kernel.
+__global__ void __launch_bounds__(128) haven_condition_kernel(
+    const __grid_constant__ LightingBatch B, const float *__restrict__ earth,
+    float sunlight_threshold, float earth_threshold, int words, int words_per_thread,
+    uint32_t *__restrict__ low_bits, uint32_t *__restrict__ outage_bits) {
+    const int tile = blockIdx.z;
+    const int index = blockIdx.x * blockDim.x + threadIdx.x;
+    if (index >= kPatch * kPatch) return;
+    const TileGeo &g = B.tiles[tile];
+    const int sample = index % kPatch, line = index / kPatch;
+    const size_t plane = static_cast<size_t>(kPatch) * kPatch;
+    const size_t base = static_cast<size_t>(tile) * words * plane + index;
+    const int w0 = blockIdx.y * words_per_thread;
+    const int w1 = min(w0 + words_per_thread, words);
+    if (sample >= g.valid_width || line >= g.valid_height) {
+        for (int w = w0; w < w1; ++w) {
+            low_bits[base + w * plane] = 0u;
+            outage_bits[base + w * plane] = 0u;
+        }
+        return;
+    }
+    Frame32 f;
+    const float *src = B.frames + (static_cast<size_t>(tile) * plane + index) * 12;
+#pragma unroll
+    for (int k = 0; k < 12; ++k) f.v[k] = src[k];
+    const float *horizon = B.horizons + (static_cast<size_t>(tile) * plane + index) * kAzimuths;
+    for (int w = w0; w < w1; ++w) {
+        uint32_t low = 0u, outage = 0u;
+        for (int j = 0; j < 32; ++j) {
+            const int t = w * 32 + j;
+            if (t >= B.time_count) break;
+            const float *v = B.vectors + 3 * static_cast<size_t>(t);
+            float azimuth_deg, elevation;
+            body_direction(f, __ldg(v), __ldg(v + 1), __ldg(v + 2), azimuth_deg, elevation);
+            low |= static_cast<uint32_t>(sun_fraction(horizon, azimuth_deg, elevation) <
+                                         sunlight_threshold) << j;
+            const float *e = earth + 3 * static_cast<size_t>(t);
+            body_direction(f, __ldg(e), __ldg(e + 1), __ldg(e + 2), azimuth_deg, elevation);
+            outage |= static_cast<uint32_t>(horizon_margin(horizon, azimuth_deg, elevation) <
+                                            earth_threshold) << j;
+        }
+        low_bits[base + w * plane] = low;
+        outage_bits[base + w * plane] = outage;
+    }
+}
+
+// Per-pixel safe-haven reducer (safe_haven.py:75-243), one thread per pixel
+// over the condition bits in time order.  The reference credits a low-Sun run
+// to every month band in which one of its samples saw an Earth outage, with
+// the run's length at each of its samples; run lengths only grow, so the
+// credit equals the run's final (or right-censored) length, applied once
+// when the run ends.  Per band the scratch holds the longest credited run and
+// flags 1 (an outage sample), 2 (a sample without outage), 4 (the current run
+// touched this band); the flags of the band in use are gathered in a
+// register and stored when the band changes or a run ends.  Output: band
+// hours = float32(longest) * float32(time_step_hours), NaN where the band saw
+// no outage or nothing else (safe_haven.py:231-240) and outside the valid
+// rectangle.
+struct HavenParams {
+    const uint32_t *low, *outage;  // [tiles, words, 16384]
+    const int *month;              // [T] band of each time step, -1 for none
+    int *longest;                  // [tiles, bands, 16384] scratch
+    uint8_t *flags;                // [tiles, bands, 16384] scratch
+    float *out;                    // [tiles, bands, 16384]
+    float hours;
+    int words, time_count, bands;
+    int2 valid[kMaxBatchTiles];
+};
+
+__global__ void __launch_bounds__(128) haven_kernel(const __grid_constant__ HavenParams P) {
+    const int tile = blockIdx.y;
+    const int index = blockIdx.x * blockDim.x + threadIdx.x;
+    if (index >= kPatch * kPatch) return;
+    const size_t plane = static_cast<size_t>(kPatch) * kPatch;
+    const size_t band0 = static_cast<size_t>(tile) * P.bands * plane + index;
+    int *longest = P.longest + band0;
+    uint8_t *flags = P.flags + band0;
+    float *out = P.out + band0;
+    const bool valid = index % kPatch < P.valid[tile].x && index / kPatch < P.valid[tile].y;
+    if (!valid) {
+        for (int b = 0; b < P.bands; ++b) out[b * plane] = __int_as_float(0x7fffffff);
+        return;
+    }
+    for (int b = 0; b < P.bands; ++b) {
+        longest[b * plane] = 0;
+        flags[b * plane] = 0;
+    }
+    int run = 0;
+    int lo = P.bands, hi = -1;       // bands the current run touched lie in [lo, hi]
+    int cached = -1;                 // band whose flags sit in `bits`
+    unsigned bits = 0u;
+    auto store = [&]() {
+        if (cached >= 0 && bits) flags[cached * plane] |= static_cast<uint8_t>(bits);
+        bits = 0u;
+    };
+    auto credit = [&]() {
+        store();
+        for (int b = lo; b <= hi; ++b) {
+            const unsigned f = flags[b * plane];
+            if (f & 4u) {
+                longest[b * plane] = max(longest[b * plane], run);
+                flags[b * plane] = static_cast<uint8_t>(f & ~4u);
+            }
+        }
+        lo = P.bands;
+        hi = -1;
+    };
+    const size_t word0 = static_cast<size_t>(tile) * P.words * plane + index;
+    for (int w = 0; w < P.words; ++w) {
+        const uint32_t low_word = __ldg(P.low + word0 + w * plane);
+        const uint32_t outage_word = __ldg(P.outage + word0 + w * plane);
+        const int steps = min(32, P.time_count - w * 32);
+        for (int j = 0; j < steps; ++j) {
+            const bool low = (low_word >> j) & 1u;
+            const bool outage = (outage_word >> j) & 1u;
+            if (low) {
+                ++run;
+            } else {
+                if (hi >= 0) credit();
+                run = 0;
+            }
+            const int m = __ldg(P.month + w * 32 + j);
+            if (m >= 0) {
+                if (m != cached) {
+                    store();
+                    cached = m;
+                }
+                bits |= outage ? 1u : 2u;
+                if (outage && low) {
+                    bits |= 4u;
+                    lo = min(lo, m);
+                    hi = max(hi, m);
+                }
+            }
+        }
+    }
+    if (hi >= 0) credit();  // the run still open at the end is right-censored
+    store();
+    for (int b = 0; b < P.bands; ++b) {
+        const unsigned f = flags[b * plane];
+        out[b * plane] = (f & 3u) == 3u
+                             ? __fmul_rn(__int2float_rn(longest[b * plane]), P.hours)
+                             : __int_as_float(0x7fffffff);
+    }
+}
+
+void safe_haven_launch(ls200_context *ctx, LightingBatch &B, int tiles, const float *earth,
+                       float sunlight_threshold, float earth_threshold, uint32_t *bits,
+                       const int *month, int bands, float hours, int *longest,
+                       uint8_t *flags, float *out) {
+    LS_REQUIRE(tiles >= 1 && tiles <= kMaxBatchTiles, "1 to 32 tiles per launch");
+    ensure_lighting_constants(ctx);
+    dim3 grid_frames(kPatch * kPatch / 128, tiles);
+    frames_kernel<<<grid_frames, 128, 0, ctx->stream>>>(B);
+    LS_CUDA(cudaGetLastError());
+    const int words = (B.time_count + 31) / 32;
+    const int chunk_steps = lighting_chunk(ctx, tiles, B.time_count);
+    const int words_per_thread = std::max(1, chunk_steps / 32);
+    const size_t stream_words = static_cast<size_t>(tiles) * words * kPatch * kPatch;
+    dim3 grid(kPatch * kPatch / 128, (words + words_per_thread - 1) / words_per_thread, tiles);
+    haven_condition_kernel<<<grid, 128, 0, ctx->stream>>>(B, earth, sunlight_threshold,
+                                                          earth_threshold, words,
+                                                          words_per_thread, bits,
+                                                          bits + stream_words);
+    LS_CUDA(cudaGetLastError());
+    HavenParams P{};
+    P.low = bits;
+    P.outage = bits + stream_words;
+    P.month = month;
+    P.longest = longest;
+    P.flags = flags;
+    P.out = out;
+    P.hours = hours;
+    P.words = words;
+    P.time_count = B.time_count;
+    P.bands = bands;
+    for (int t = 0; t < tiles; ++t)
+        P.valid[t] = make_int2(B.tiles[t].valid_width, B.tiles[t].valid_height);
+    haven_kernel<<<dim3(kPatch * kPatch / 128, tiles), 128, 0, ctx->stream>>>(P);
+    LS_CUDA(cudaGetLastError());
+}
+
 void sun_fraction_launch(ls200_context *ctx, const float *horizons, const float *azimuth_deg,
                          const float *elevation_deg, int n, float *out) {
     ensure_lighting_constants(ctx);

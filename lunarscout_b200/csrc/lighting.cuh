@@ -60,6 +60,17 @@ void mission_duration_launch(ls200_context *ctx, LightingBatch &batch, int tiles
                              uint32_t *bits, const double *hours, const double *prefix,
                              const int2 *windows, int interval_count, bool days, float *out);
 
+// The safe-haven product fused with the lighting: low-Sun and Earth-outage
+// bits ([2, tiles, ceil(T/32), 16384] words in `bits`), then per pixel and
+// month band the longest low-Sun run that overlapped an outage in that band,
+// in hours, into out [tiles, bands, 16384] (NaN where the band is ill-posed).
+// month: device [T] band index per time step (-1 for none); longest and
+// flags: device scratch [tiles, bands, 16384].
+void safe_haven_launch(ls200_context *ctx, LightingBatch &batch, int tiles, const float *earth,
+                       float sunlight_threshold, float earth_threshold, uint32_t *bits,
+                       const int *month, int bands, float hours, int *longest,
+                       uint8_t *flags, float *out);
+
 #ifdef LS200_LIGHTING_KERNELS
 // Slice half-heights and their normaliser (set by ensure_lighting_constants).
 __constant__ float c_half_circle[16];

@@ -9,6 +9,7 @@ namespace ls200 {
 struct LightingState {
     DeviceBuffer dem, horizons, frames, out;
     DeviceBuffer duration_frames, duration_bits, duration_tables;  // mission duration
+    DeviceBuffer haven_bits, haven_months, haven_longest, haven_flags;  // safe haven
     TileGeo geo{};
     bool loaded = false;
     std::set<ls200_vectors *> vectors;  // live vector tables of the context
@@ -283,6 +284,71 @@ ls200_status ls200_mission_duration_device(
                                 d_hours, integral ? d_prefix : nullptr, d_windows,
                                 interval_count, output_days != 0, out);
         // The host tables above must outlive their copies.
+        LS_CUDA(cudaStreamSynchronize(ctx->stream));
+    });
+}
+
+ls200_status ls200_safe_haven_device(
+    ls200_context *ctx, int tile_count, const float *patch_dems, const double *geo_transforms,
+    const double *projections, const int32_t *windows, const float *horizons,
+    const ls200_vectors *sun, const ls200_vectors *earth, float sunlight_threshold,
+    float earth_threshold_deg, float time_step_hours, const int32_t *month_index_of,
+    int band_count, float *out) {
+    return guard([&] {
+        LS_REQUIRE(ctx && patch_dems && geo_transforms && projections && windows && horizons &&
+                       sun && earth && month_index_of && out,
+                   "NULL argument");
+        LS_REQUIRE(tile_count >= 1 && tile_count <= kMaxBatchTiles,
+                   "tile_count must be between 1 and 32");
+        LS_REQUIRE(sun->ctx == ctx && earth->ctx == ctx && sun->count > 0,
+                   "vectors belong to another context");
+        LS_REQUIRE(earth->count == sun->count,
+                   "earth vectors must match the sun vectors' time axis");
+        LS_REQUIRE(sunlight_threshold >= 0.0f && sunlight_threshold <= 1.0f,
+                   "sunlight_threshold must be between zero and one");
+        LS_REQUIRE(std::isfinite(earth_threshold_deg), "earth_threshold_deg must be finite");
+        LS_REQUIRE(std::isfinite(time_step_hours) && time_step_hours > 0.0f,
+                   "time_step_hours must be positive and finite");
+        LS_REQUIRE(band_count >= 1 && band_count <= 65536,
+                   "band_count must be between 1 and 65536");
+        const int count = sun->count;
+        for (int t = 0; t < count; ++t)
+            LS_REQUIRE(month_index_of[t] >= -1 && month_index_of[t] < band_count,
+                       "month indices must be -1 or a band index");
+        std::lock_guard<std::mutex> hold(ctx->lock);
+        activate(ctx);
+        LightingState &st = state_of(ctx);
+        LightingBatch B{};
+        for (int t = 0; t < tile_count; ++t) {
+            std::memcpy(B.tiles[t].gt, geo_transforms + 6 * t, sizeof B.tiles[t].gt);
+            std::memcpy(B.tiles[t].proj, projections + 6 * t, sizeof B.tiles[t].proj);
+            B.tiles[t].tile_x = windows[4 * t + 0];
+            B.tiles[t].tile_y = windows[4 * t + 1];
+            B.tiles[t].valid_width = windows[4 * t + 2];
+            B.tiles[t].valid_height = windows[4 * t + 3];
+            check_valid(B.tiles[t].valid_width, B.tiles[t].valid_height);
+        }
+        const size_t plane = static_cast<size_t>(kPatch) * kPatch;
+        const size_t words = (static_cast<size_t>(count) + 31) / 32;
+        const size_t cells = static_cast<size_t>(tile_count) * band_count * plane;
+        st.duration_frames.reserve(sizeof(float) * 12 * tile_count * plane);
+        st.haven_bits.reserve(sizeof(uint32_t) * 2 * tile_count * words * plane);
+        st.haven_months.reserve(sizeof(int32_t) * count);
+        st.haven_longest.reserve(sizeof(int32_t) * cells);
+        st.haven_flags.reserve(cells);
+        LS_CUDA(cudaMemcpyAsync(st.haven_months.as<int32_t>(), month_index_of,
+                                sizeof(int32_t) * count, cudaMemcpyHostToDevice, ctx->stream));
+        B.patch_dem = patch_dems;
+        B.horizons = horizons;
+        B.vectors = sun->data;
+        B.frames = st.duration_frames.as<float>();
+        B.time_start = 0;
+        B.time_count = count;
+        safe_haven_launch(ctx, B, tile_count, earth->data, sunlight_threshold,
+                          earth_threshold_deg, st.haven_bits.as<uint32_t>(),
+                          st.haven_months.as<int32_t>(), band_count, time_step_hours,
+                          st.haven_longest.as<int32_t>(), st.haven_flags.as<uint8_t>(), out);
+        // The host month table must outlive its copy.
         LS_CUDA(cudaStreamSynchronize(ctx->stream));
     });
 }

@@ -228,6 +228,69 @@ class LightmapCudaSession:
         grid = out.cpu().numpy().reshape(len(windows), PATCH_SIZE, PATCH_SIZE)
         return np.ascontiguousarray(grid[:, :valid_height, :valid_width])
 
+    def safe_haven_durations(self, dem, horizons_deg, sun_vectors_m, earth_vectors_m, *,
+                             tile_y: int, tile_x: int, valid_height: int, valid_width: int,
+                             month_index_of, band_count: int, time_step_hours: float,
+                             sunlight_threshold: float = 0.2,
+                             earth_threshold_deg: float = 2.0) -> tuple[np.ndarray, ...]:
+        """Per month band, the longest low-Sun run (fraction <
+        ``sunlight_threshold``) that overlapped an Earth outage (margin <
+        ``earth_threshold_deg``) in that band, times ``time_step_hours``:
+        float32 ``[valid_height, valid_width]`` per band, NaN where the band
+        saw no outage or only outages (reduce_safe_haven_patch_stream,
+        safe_haven.py:75-243, over the streams of safe_haven_pipeline.py:240-272,
+        evaluated and reduced on the device).  ``month_index_of`` int32[T]
+        gives each time step's band (-1 for none)."""
+        import torch
+
+        sun = np.ascontiguousarray(validate_vectors(sun_vectors_m), dtype=np.float32)
+        earth = np.ascontiguousarray(validate_vectors(earth_vectors_m), dtype=np.float32)
+        if len(earth) != len(sun):
+            raise ValueError("timestamps, Sun vectors, and Earth vectors must align")
+        if not 0.0 <= sunlight_threshold <= 1.0:
+            raise ValueError("sunlight_threshold must be between zero and one")
+        if not np.isfinite(earth_threshold_deg):
+            raise ValueError("earth_threshold_deg must be finite")
+        if not np.isfinite(time_step_hours) or time_step_hours <= 0.0:
+            raise ValueError("time_step_hours must be positive and finite")
+        if isinstance(band_count, bool) or not isinstance(band_count, (int, np.integer)) \
+                or band_count < 1:
+            raise ValueError("band_count must be a positive integer")
+        months = np.ascontiguousarray(month_index_of, dtype=np.int32)
+        if months.shape != (len(sun),):
+            raise ValueError("month_index_of must have shape (time_count,)")
+        if np.any((months < -1) | (months >= band_count)):
+            raise ValueError("month indices must be -1 or a band index")
+        horizons = np.ascontiguousarray(horizons_deg, dtype=np.float32)
+        if horizons.shape != (PATCH_SIZE, PATCH_SIZE, AZIMUTH_COUNT):
+            raise ValueError("horizons must have shape (128, 128, 1440)")
+        if not 1 <= valid_width <= PATCH_SIZE or not 1 <= valid_height <= PATCH_SIZE:
+            raise ValueError("valid patch dimensions must be between 1 and 128")
+        patch = torch.from_numpy(
+            patch_elevations(dem, tile_y, tile_x, valid_height, valid_width)).cuda()
+        device_horizons = torch.from_numpy(horizons).cuda()
+        out = torch.empty((int(band_count), PATCH_SIZE * PATCH_SIZE), dtype=torch.float32,
+                          device="cuda")
+        geo = np.ascontiguousarray(dem.geo_transform, dtype=np.float64)
+        projection = projection_array(dem.projection)
+        window = np.array([tile_x, tile_y, valid_width, valid_height], dtype=np.int32)
+        torch.cuda.synchronize()
+        with self._lock, self._context.lock:
+            sun_table = DeviceVectors(self._context.handle, sun)
+            earth_table = DeviceVectors(self._context.handle, earth)
+            try:
+                call("ls200_safe_haven_device", self._context.handle, 1,
+                     ctypes.c_void_p(patch.data_ptr()), geo.ctypes.data, projection.ctypes.data,
+                     window.ctypes.data, ctypes.c_void_p(device_horizons.data_ptr()),
+                     sun_table.handle, earth_table.handle, float(sunlight_threshold),
+                     float(earth_threshold_deg), float(np.float32(time_step_hours)),
+                     months.ctypes.data, int(band_count), ctypes.c_void_p(out.data_ptr()))
+            finally:
+                sun_table.close()
+                earth_table.close()
+        grid = out.cpu().numpy().reshape(int(band_count), PATCH_SIZE, PATCH_SIZE)
+        return tuple(np.ascontiguousarray(band[:valid_height, :valid_width]) for band in grid)
+
     def sun_fraction(self, horizons: np.ndarray, azimuth_deg, elevation_deg) -> np.ndarray:
         """Diagnostic: fraction of the disk at (azimuth, elevation) above each
         horizon row (lightmap.py:32-73)."""

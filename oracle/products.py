@@ -193,6 +193,45 @@ def longest_duration(condition: np.ndarray, sample_hours: np.ndarray,
     return np.maximum(longest, current)
 
 
+def safe_haven(fractions: np.ndarray, margins: np.ndarray, month_index_of: np.ndarray,
+               band_count: int, *, sunlight_threshold: float, earth_threshold_deg: float,
+               time_step_hours: float) -> np.ndarray:
+    """Per-band safe-haven hours, float32[B, H, W] with NaN nodata
+    (safe_haven.py:75-243), stepping through time as the reference does.
+
+    fractions, margins float32[T, H, W]; month_index_of int32[T] (-1: none).
+    Per step: the low-Sun run length grows or resets (:180); the step's band
+    records an outage or not and marks the run when it is low-Sun during an
+    outage (:184-189); every marked band takes the run length while the run
+    lasts, and marks clear when it ends (:194-201).  Bands without an outage,
+    or without a non-outage sample, are NaN (:231-240).
+    """
+    fractions = np.asarray(fractions, dtype=np.float32)
+    margins = np.asarray(margins, dtype=np.float32)
+    count, height, width = fractions.shape
+    shape = (height, width)
+    run = np.zeros(shape, dtype=np.int32)
+    touching = np.zeros((band_count, *shape), dtype=bool)
+    best = np.zeros((band_count, *shape), dtype=np.int32)
+    outage_seen = np.zeros((band_count, *shape), dtype=bool)
+    above_seen = np.zeros((band_count, *shape), dtype=bool)
+    for t in range(count):
+        low = fractions[t] < np.float32(sunlight_threshold)
+        outage = margins[t] < np.float32(earth_threshold_deg)
+        run = np.where(low, run + 1, 0).astype(np.int32)
+        band = int(month_index_of[t])
+        if band >= 0:
+            above_seen[band] |= ~outage
+            outage_seen[band] |= outage
+            touching[band] |= outage & low
+        for b in range(band_count):
+            best[b] = np.maximum(best[b], np.where(touching[b] & low, run, 0))
+            touching[b] &= low
+    out = best.astype(np.float32) * np.float32(time_step_hours)
+    out[~outage_seen | ~above_seen] = np.nan
+    return out
+
+
 _SHORT_SCALE = np.float32(32767.0) / np.float32(50.0)
 _ELEVATION_SCALE = np.float32(50.0) / np.float32(32767.0)
 

@@ -16,6 +16,9 @@ pyproj/rasterio, absent here) and extracts:
 * pyramids.npz — C# pyramid captures incl. the NaN/inf/-20000 fixture.
 * segments_halo.npz — the 16x16-tile, 16-azimuth, two-DEM halo fixture: the
   C# segment tensor, the reference's Numba segment tensor and its DEMs.
+* safe_haven_reference.npz — the reference safe-haven reducer and month-band
+  helpers on the reference CPU backend's lighting streams and on seeded
+  synthetic streams (safe_haven_reference below).
 
 Usage: python tests/golden/make_golden.py [--simulate]
 (--simulate re-runs the simulator capture, ~5 min).
@@ -353,6 +356,73 @@ def lighting_reference() -> None:
     )
 
 
+def safe_haven_reference() -> None:
+    """The reference safe-haven reducer and its month-band helpers on (a) the
+    reference CPU backend's fraction / Earth-margin tiles of
+    lighting_reference.npz and (b) seeded synthetic streams over four months,
+    with a second mapping whose first month is left out (-1) and whose times
+    are not in order."""
+    import datetime as dt
+
+    from lunarscout._numba_horizon.safe_haven import (
+        _month_indices_map, build_month_bands, reduce_safe_haven_patch_stream)
+
+    def run(fractions, margins, months, bands, sunlight, earth, hours):
+        out = reduce_safe_haven_patch_stream(
+            iter(fractions), iter(margins), len(fractions), bands, month_index_of=months,
+            sunlight_threshold=sunlight, earth_threshold_deg=earth, time_step_hours=hours)
+        return np.stack(out)
+
+    lighting = np.load(OUT / "lighting_reference.npz")
+    start = dt.datetime(2029, 1, 1, tzinfo=dt.timezone.utc)
+    times_a = [start + dt.timedelta(hours=float(h)) for h in lighting["hours"]]
+    bands_a = build_month_bands(times_a)
+    months_a = _month_indices_map(times_a, bands_a)
+    fractions_a = lighting["fractions"]
+    margins_a = lighting["margins"]
+    sunlight_a = 0.5
+    earth_a = float(np.median(margins_a))
+    out_a = run(fractions_a, margins_a, months_a, bands_a, sunlight_a, earth_a, 6.0)
+
+    rng = np.random.default_rng(20290120)
+    count, height, width = 300, 12, 10
+    first = dt.datetime(2029, 1, 20, 3, tzinfo=dt.timezone.utc)
+    times_b = [first + dt.timedelta(hours=6 * i) for i in range(count)]
+    low = np.zeros((count, height, width), dtype=bool)
+    state = rng.random((height, width)) < 0.5
+    for t in range(count):
+        state ^= rng.random((height, width)) < 0.08
+        low[t] = state
+    fractions_b = np.where(low, rng.uniform(0.0, 0.19, low.shape),
+                           rng.uniform(0.21, 1.0, low.shape)).astype(np.float32)
+    walk = np.cumsum(rng.normal(0.0, 0.6, (count, height, width)), axis=0)
+    margins_b = (2.0 + walk - walk.mean(axis=0)).astype(np.float32)
+    margins_b[:, 0, :3] = 5.0        # never an outage: NaN
+    margins_b[:, 1, :3] = -1.0       # always an outage: NaN
+    margins_b[:, 2, 0] = np.float32(2.0)  # exactly at the threshold: not an outage
+    fractions_b[:, 3, 0] = np.float32(0.2)  # exactly at the threshold: not low
+    bands_b = build_month_bands(times_b)
+    months_b = _month_indices_map(times_b, bands_b)
+    out_b = run(fractions_b, margins_b, months_b, bands_b, 0.2, 2.0, 6.0)
+
+    order = np.arange(count)
+    order[40:60] = order[40:60][::-1]
+    times_c = [times_b[i] for i in order]
+    bands_c = bands_b[1:]
+    months_c = _month_indices_map(times_c, bands_c)
+    out_c = run(fractions_b, margins_b, months_c, bands_c, 0.2, 2.0, 1.5)
+
+    iso = lambda values: np.array([v.isoformat() for v in values])
+    np.savez_compressed(
+        OUT / "safe_haven_reference.npz",
+        a_months=months_a, a_bands=iso([b for band in bands_a for b in band]),
+        a_sunlight=np.float64(sunlight_a), a_earth=np.float64(earth_a), a_out=out_a,
+        b_times=iso(times_b), b_fractions=fractions_b, b_margins=margins_b, b_months=months_b,
+        b_bands=iso([b for band in bands_b for b in band]), b_out=out_b,
+        c_times=iso(times_c), c_months=months_c, c_out=out_c,
+    )
+
+
 def codec_reference() -> None:
     """The reference .cbin encoder on a deterministic degree tile."""
     import hashlib
@@ -388,6 +458,7 @@ def main() -> None:
         "lighting_csharp": lighting_csharp,
         "lighting_reference": lighting_reference,
         "codec": codec_reference,
+        "safe_haven": safe_haven_reference,
     }
     for name, job in jobs.items():
         if args.only and name not in args.only.split(","):

@@ -194,3 +194,81 @@ def test_mission_durations_against_the_reference_cpu_chain(lighting_session, sit
     near = (np.abs(cpu - np.float32(0.5)) <= 1e-4).any(axis=0)
     assert np.all(near[differ.any(axis=0)])
     assert differ.mean() <= 0.01
+
+
+@pytest.fixture(scope="module")
+def haven(lighting_session, site):
+    from datetime import datetime, timedelta, timezone
+
+    from lunarscout_b200 import synthetic
+    from lunarscout_b200.safe_haven import month_bands, month_indices
+
+    hours = synthetic.hours_between("2029-01-20T00", "2029-04-10T00", 3.0)
+    start = datetime(2029, 1, 20, tzinfo=timezone.utc)
+    times = [start + timedelta(hours=float(h)) for h in hours]
+    bands = month_bands(times)
+    sun, earth = synthetic.sun_vectors(hours), synthetic.earth_vectors(hours)
+    fractions = np.stack(list(lighting_session.iter_patch_fraction_tiles(
+        site["dem"], site["horizons"], sun, **site["tile"])))
+    margins = np.stack(list(lighting_session.iter_patch_margin_tiles(
+        site["dem"], site["horizons"], earth, **site["tile"])))
+    return dict(times=times, bands=bands, months=month_indices(times, bands), sun=sun,
+                earth=earth, fractions=fractions, margins=margins)
+
+
+def test_safe_haven_reduces_the_device_streams_exactly(lighting_session, site, haven):
+    assert len(haven["bands"]) == 4
+    cases = [(0.2, 2.0), (0.5, float(np.quantile(haven["margins"], 0.3)))]
+    for sunlight, earth_deg in cases:
+        got = lighting_session.safe_haven_durations(
+            site["dem"], site["horizons"], haven["sun"], haven["earth"],
+            month_index_of=haven["months"], band_count=len(haven["bands"]),
+            time_step_hours=3.0, sunlight_threshold=sunlight, earth_threshold_deg=earth_deg,
+            **site["tile"])
+        expected = products.safe_haven(haven["fractions"], haven["margins"], haven["months"],
+                                       len(haven["bands"]), sunlight_threshold=sunlight,
+                                       earth_threshold_deg=earth_deg, time_step_hours=3.0)
+        got = np.stack(got)
+        assert got.shape == (4, 40, 48)
+        np.testing.assert_array_equal(got, expected)
+    assert np.isnan(got).any() and (got[np.isfinite(got)] > 0).any()
+
+
+def test_safe_haven_unordered_months_and_the_patch_helper(lighting_session, site, haven):
+    from lunarscout_b200.safe_haven import safe_haven_patch
+
+    months = haven["months"].copy()
+    months[100:300] = months[100:300][::-1]
+    months[::7] = -1
+    earth_deg = float(np.quantile(haven["margins"], 0.5))
+    got = np.stack(lighting_session.safe_haven_durations(
+        site["dem"], site["horizons"], haven["sun"], haven["earth"], month_index_of=months,
+        band_count=4, time_step_hours=0.75, sunlight_threshold=0.5,
+        earth_threshold_deg=earth_deg, **site["tile"]))
+    expected = products.safe_haven(haven["fractions"], haven["margins"], months, 4,
+                                   sunlight_threshold=0.5, earth_threshold_deg=earth_deg,
+                                   time_step_hours=0.75)
+    np.testing.assert_array_equal(got, expected)
+    bands, durations = safe_haven_patch(lighting_session, site["dem"], site["horizons"],
+                                        haven["times"], haven["sun"], haven["earth"],
+                                        time_step_hours=3.0, **site["tile"])
+    assert bands == haven["bands"]
+    expected = products.safe_haven(haven["fractions"], haven["margins"], haven["months"], 4,
+                                   sunlight_threshold=0.2, earth_threshold_deg=2.0,
+                                   time_step_hours=3.0)
+    np.testing.assert_array_equal(np.stack(durations), expected)
+
+
+def test_safe_haven_validation(lighting_session, site, haven):
+    common = dict(month_index_of=haven["months"], band_count=4, time_step_hours=3.0,
+                  **site["tile"])
+    args = (site["dem"], site["horizons"], haven["sun"], haven["earth"])
+    for bad in (dict(sunlight_threshold=1.5), dict(earth_threshold_deg=float("nan")),
+                dict(time_step_hours=0.0), dict(band_count=0),
+                dict(month_index_of=haven["months"][:-1]),
+                dict(month_index_of=np.full_like(haven["months"], 4))):
+        with pytest.raises(ValueError):
+            lighting_session.safe_haven_durations(*args, **{**common, **bad})
+    with pytest.raises(ValueError):
+        lighting_session.safe_haven_durations(site["dem"], site["horizons"], haven["sun"],
+                                              haven["earth"][:-1], **common)

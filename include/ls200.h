@@ -305,6 +305,19 @@ ls200_status ls200_safe_haven_device(
     const ls200_vectors *sun, const ls200_vectors *earth, float sunlight_threshold,
     float earth_threshold_deg, float time_step_hours, const int32_t *month_index_of,
     int band_count, float *out);
+/* ---- Earth-visibility fraction: mean over time of (Earth margin >=
+ *      threshold), the margin being iter_patch_margin_tiles'
+ *      (src/lunarscout/_numba_horizon/lightmap_cuda.py:125-145,
+ *      lightmap_cpu.py:121-141) for the Earth vectors ----
+ * Tiles as in ls200_lighting_device; earth: vector table of T steps.  out
+ * (device) float32 [tiles, 16384]: count / T per pixel (FP64 division rounded
+ * to float32), NaN outside each tile's valid rectangle. */
+ls200_status ls200_earth_visibility_device(ls200_context *ctx, int tile_count,
+                                           const float *patch_dems,
+                                           const double *geo_transforms,
+                                           const double *projections, const int32_t *windows,
+                                           const float *horizons, const ls200_vectors *earth,
+                                           float threshold_deg, float *out);
 /* Diagnostic: sun fraction at given (azimuth, elevation) in degrees for n
  * horizon rows float32[n,1440] (lightmap.py:32-73). */
 ls200_status ls200_sun_fraction(ls200_context *ctx, const float *horizons,

@@ -102,6 +102,7 @@ SIGNATURES: dict[str, list] = {
                                       _vp, _i, _i, _vp],
     "ls200_safe_haven_device": [_vp, _i, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _f, _f, _f, _vp,
                                 _i, _vp],
+    "ls200_earth_visibility_device": [_vp, _i, _vp, _vp, _vp, _vp, _vp, _vp, _f, _vp],
     "ls200_set_batch_config": [_vp, _i, _i],
     "ls200_get_batch_config": [_vp, _vp, _vp],
     "ls200_cbin_encode": [_vp, _f32p, _vp, _i64, _vp],

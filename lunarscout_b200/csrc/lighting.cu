@@ -597,6 +597,65 @@ void safe_haven_launch(ls200_context *ctx, LightingBatch &B, int tiles, const fl
     LS_CUDA(cudaGetLastError());
 }
 
+// Earth-visibility fraction: per pixel, the share of time steps whose Earth
+// margin (the a13 signal of lighting_kernel, lightmap_cpu.py:121-141) is >=
+// threshold.  Each thread counts its pixel over one time chunk and adds the
+// count to the pixel's counter; visibility_finalize divides by T (FP64, then
+// rounded to float32).
+__global__ void __launch_bounds__(128) visibility_kernel(const __grid_constant__ LightingBatch B,
+                                                         float threshold,
+                                                         unsigned *__restrict__ counts) {
+    const int tile = blockIdx.z;
+    const int index = blockIdx.x * blockDim.x + threadIdx.x;
+    if (index >= kPatch * kPatch) return;
+    const TileGeo &g = B.tiles[tile];
+    if (index % kPatch >= g.valid_width || index / kPatch >= g.valid_height) return;
+    const size_t plane = static_cast<size_t>(kPatch) * kPatch;
+    const int t0 = blockIdx.y * B.chunk;
+    const int t1 = min(t0 + B.chunk, B.time_count);
+    Frame32 f;
+    const float *src = B.frames + (static_cast<size_t>(tile) * plane + index) * 12;
+#pragma unroll
+    for (int k = 0; k < 12; ++k) f.v[k] = src[k];
+    const float *horizon = B.horizons + (static_cast<size_t>(tile) * plane + index) * kAzimuths;
+    unsigned count = 0;
+    for (int t = t0; t < t1; ++t) {
+        const float *v = B.vectors + 3 * static_cast<size_t>(t);
+        float azimuth_deg, elevation;
+        body_direction(f, __ldg(v), __ldg(v + 1), __ldg(v + 2), azimuth_deg, elevation);
+        count += horizon_margin(horizon, azimuth_deg, elevation) >= threshold ? 1u : 0u;
+    }
+    if (count) atomicAdd(counts + static_cast<size_t>(tile) * plane + index, count);
+}
+
+__global__ void visibility_finalize(const unsigned *__restrict__ counts, int n, int time_count,
+                                    const int2 *__restrict__ valid, float *__restrict__ out) {
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const int tile = i / (kPatch * kPatch), index = i % (kPatch * kPatch);
+    const bool inside = index % kPatch < valid[tile].x && index / kPatch < valid[tile].y;
+    out[i] = inside ? static_cast<float>(static_cast<double>(counts[i]) / time_count)
+                    : __int_as_float(0x7fffffff);
+}
+
+void visibility_launch(ls200_context *ctx, LightingBatch &B, int tiles, float threshold,
+                       unsigned *counts, int2 *valid, float *out) {
+    LS_REQUIRE(tiles >= 1 && tiles <= kMaxBatchTiles, "1 to 32 tiles per launch");
+    ensure_lighting_constants(ctx);
+    const int n = tiles * kPatch * kPatch;
+    LS_CUDA(cudaMemsetAsync(counts, 0, sizeof(unsigned) * n, ctx->stream));
+    dim3 grid_frames(kPatch * kPatch / 128, tiles);
+    frames_kernel<<<grid_frames, 128, 0, ctx->stream>>>(B);
+    LS_CUDA(cudaGetLastError());
+    B.chunk = lighting_chunk(ctx, tiles, B.time_count);
+    dim3 grid(kPatch * kPatch / 128, (B.time_count + B.chunk - 1) / B.chunk, tiles);
+    visibility_kernel<<<grid, 128, 0, ctx->stream>>>(B, threshold, counts);
+    LS_CUDA(cudaGetLastError());
+    visibility_finalize<<<(n + 255) / 256, 256, 0, ctx->stream>>>(counts, n, B.time_count, valid,
+                                                                  out);
+    LS_CUDA(cudaGetLastError());
+}
+
 void sun_fraction_launch(ls200_context *ctx, const float *horizons, const float *azimuth_deg,
                          const float *elevation_deg, int n, float *out) {
     ensure_lighting_constants(ctx);

@@ -71,6 +71,13 @@ void safe_haven_launch(ls200_context *ctx, LightingBatch &batch, int tiles, cons
                        const int *month, int bands, float hours, int *longest,
                        uint8_t *flags, float *out);
 
+// Earth-visibility fraction: per pixel the share of the batch's time steps
+// whose Earth margin is >= threshold (degrees), into out [tiles, 16384] (NaN
+// outside the valid rectangle).  counts: device scratch [tiles, 16384];
+// valid: device [tiles] (valid width, valid height).
+void visibility_launch(ls200_context *ctx, LightingBatch &batch, int tiles, float threshold,
+                       unsigned *counts, int2 *valid, float *out);
+
 #ifdef LS200_LIGHTING_KERNELS
 // Slice half-heights and their normaliser (set by ensure_lighting_constants).
 __constant__ float c_half_circle[16];

@@ -10,6 +10,7 @@ struct LightingState {
     DeviceBuffer dem, horizons, frames, out;
     DeviceBuffer duration_frames, duration_bits, duration_tables;  // mission duration
     DeviceBuffer haven_bits, haven_months, haven_longest, haven_flags;  // safe haven
+    DeviceBuffer visibility;  // Earth visibility: counts, then the valid table
     TileGeo geo{};
     bool loaded = false;
     std::set<ls200_vectors *> vectors;  // live vector tables of the context
@@ -349,6 +350,55 @@ ls200_status ls200_safe_haven_device(
                           st.haven_months.as<int32_t>(), band_count, time_step_hours,
                           st.haven_longest.as<int32_t>(), st.haven_flags.as<uint8_t>(), out);
         // The host month table must outlive its copy.
+        LS_CUDA(cudaStreamSynchronize(ctx->stream));
+    });
+}
+
+ls200_status ls200_earth_visibility_device(ls200_context *ctx, int tile_count,
+                                           const float *patch_dems,
+                                           const double *geo_transforms,
+                                           const double *projections, const int32_t *windows,
+                                           const float *horizons, const ls200_vectors *earth,
+                                           float threshold_deg, float *out) {
+    return guard([&] {
+        LS_REQUIRE(ctx && patch_dems && geo_transforms && projections && windows && horizons &&
+                       earth && out,
+                   "NULL argument");
+        LS_REQUIRE(tile_count >= 1 && tile_count <= kMaxBatchTiles,
+                   "tile_count must be between 1 and 32");
+        LS_REQUIRE(earth->ctx == ctx && earth->count > 0, "earth vectors belong to another context");
+        LS_REQUIRE(std::isfinite(threshold_deg), "threshold_deg must be finite");
+        std::lock_guard<std::mutex> hold(ctx->lock);
+        activate(ctx);
+        LightingState &st = state_of(ctx);
+        LightingBatch B{};
+        std::vector<int2> valid(tile_count);
+        for (int t = 0; t < tile_count; ++t) {
+            std::memcpy(B.tiles[t].gt, geo_transforms + 6 * t, sizeof B.tiles[t].gt);
+            std::memcpy(B.tiles[t].proj, projections + 6 * t, sizeof B.tiles[t].proj);
+            B.tiles[t].tile_x = windows[4 * t + 0];
+            B.tiles[t].tile_y = windows[4 * t + 1];
+            B.tiles[t].valid_width = windows[4 * t + 2];
+            B.tiles[t].valid_height = windows[4 * t + 3];
+            check_valid(B.tiles[t].valid_width, B.tiles[t].valid_height);
+            valid[t] = make_int2(B.tiles[t].valid_width, B.tiles[t].valid_height);
+        }
+        const size_t plane = static_cast<size_t>(kPatch) * kPatch;
+        const size_t counts_bytes = sizeof(unsigned) * tile_count * plane;
+        st.duration_frames.reserve(sizeof(float) * 12 * tile_count * plane);
+        st.visibility.reserve(counts_bytes + sizeof(int2) * kMaxBatchTiles);
+        int2 *d_valid = reinterpret_cast<int2 *>(st.visibility.as<char>() + counts_bytes);
+        LS_CUDA(cudaMemcpyAsync(d_valid, valid.data(), sizeof(int2) * tile_count,
+                                cudaMemcpyHostToDevice, ctx->stream));
+        B.patch_dem = patch_dems;
+        B.horizons = horizons;
+        B.vectors = earth->data;
+        B.frames = st.duration_frames.as<float>();
+        B.time_start = 0;
+        B.time_count = earth->count;
+        visibility_launch(ctx, B, tile_count, threshold_deg, st.visibility.as<unsigned>(),
+                          d_valid, out);
+        // The host valid table must outlive its copy.
         LS_CUDA(cudaStreamSynchronize(ctx->stream));
     });
 }

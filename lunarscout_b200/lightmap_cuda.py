@@ -291,6 +291,45 @@ class LightmapCudaSession:
         grid = out.cpu().numpy().reshape(int(band_count), PATCH_SIZE, PATCH_SIZE)
         return tuple(np.ascontiguousarray(band[:valid_height, :valid_width]) for band in grid)
 
+    def earth_visibility_fraction(self, dem, horizons_deg, earth_vectors_m, *, tile_y: int,
+                                  tile_x: int, valid_height: int, valid_width: int,
+                                  threshold_deg: float = 0.0) -> np.ndarray:
+        """Share of the time steps at which the Earth's centre stands at least
+        ``threshold_deg`` above the terrain horizon: the mean over time of
+        (margin >= threshold) for the margins ``iter_patch_margin_tiles``
+        yields (lightmap_cuda.py:125-145), float32 [valid_height,
+        valid_width], counted on the device without materialising the
+        margins."""
+        import torch
+
+        earth = np.ascontiguousarray(validate_vectors(earth_vectors_m), dtype=np.float32)
+        if not np.isfinite(threshold_deg):
+            raise ValueError("threshold_deg must be finite")
+        horizons = np.ascontiguousarray(horizons_deg, dtype=np.float32)
+        if horizons.shape != (PATCH_SIZE, PATCH_SIZE, AZIMUTH_COUNT):
+            raise ValueError("horizons must have shape (128, 128, 1440)")
+        if not 1 <= valid_width <= PATCH_SIZE or not 1 <= valid_height <= PATCH_SIZE:
+            raise ValueError("valid patch dimensions must be between 1 and 128")
+        patch = torch.from_numpy(
+            patch_elevations(dem, tile_y, tile_x, valid_height, valid_width)).cuda()
+        device_horizons = torch.from_numpy(horizons).cuda()
+        out = torch.empty(PATCH_SIZE * PATCH_SIZE, dtype=torch.float32, device="cuda")
+        geo = np.ascontiguousarray(dem.geo_transform, dtype=np.float64)
+        projection = projection_array(dem.projection)
+        window = np.array([tile_x, tile_y, valid_width, valid_height], dtype=np.int32)
+        torch.cuda.synchronize()
+        with self._lock, self._context.lock:
+            table = DeviceVectors(self._context.handle, earth)
+            try:
+                call("ls200_earth_visibility_device", self._context.handle, 1,
+                     ctypes.c_void_p(patch.data_ptr()), geo.ctypes.data, projection.ctypes.data,
+                     window.ctypes.data, ctypes.c_void_p(device_horizons.data_ptr()),
+                     table.handle, float(threshold_deg), ctypes.c_void_p(out.data_ptr()))
+            finally:
+                table.close()
+        grid = out.cpu().numpy().reshape(PATCH_SIZE, PATCH_SIZE)
+        return np.ascontiguousarray(grid[:valid_height, :valid_width])
+
     def sun_fraction(self, horizons: np.ndarray, azimuth_deg, elevation_deg) -> np.ndarray:
         """Diagnostic: fraction of the disk at (azimuth, elevation) above each
         horizon row (lightmap.py:32-73)."""

@@ -232,6 +232,15 @@ def safe_haven(fractions: np.ndarray, margins: np.ndarray, month_index_of: np.nd
     return out
 
 
+def earth_visibility(margins: np.ndarray, threshold_deg: float = 0.0) -> np.ndarray:
+    """Share of time steps with Earth margin >= threshold, float32[H, W]
+    (count / T in FP64, rounded to float32), from float32[T, H, W] margins
+    (lightmap_cpu.py:121-141 per step)."""
+    margins = np.asarray(margins, dtype=np.float32)
+    counts = np.count_nonzero(margins >= np.float32(threshold_deg), axis=0)
+    return (counts.astype(np.float64) / margins.shape[0]).astype(np.float32)
+
+
 _SHORT_SCALE = np.float32(32767.0) / np.float32(50.0)
 _ELEVATION_SCALE = np.float32(50.0) / np.float32(32767.0)
 

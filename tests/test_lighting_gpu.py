@@ -272,3 +272,28 @@ def test_safe_haven_validation(lighting_session, site, haven):
     with pytest.raises(ValueError):
         lighting_session.safe_haven_durations(site["dem"], site["horizons"], haven["sun"],
                                               haven["earth"][:-1], **common)
+
+
+def test_earth_visibility_counts_the_device_margins_exactly(lighting_session, site, haven):
+    for threshold in (0.0, float(np.quantile(haven["margins"], 0.4))):
+        got = lighting_session.earth_visibility_fraction(
+            site["dem"], site["horizons"], haven["earth"], threshold_deg=threshold,
+            **site["tile"])
+        np.testing.assert_array_equal(got, products.earth_visibility(haven["margins"],
+                                                                     threshold))
+    assert got.shape == (40, 48) and 0.0 < got.mean() < 1.0
+    with pytest.raises(ValueError):
+        lighting_session.earth_visibility_fraction(site["dem"], site["horizons"],
+                                                   haven["earth"], threshold_deg=float("inf"),
+                                                   **site["tile"])
+
+
+def test_earth_visibility_against_the_reference_cpu_margins(lighting_session, site):
+    golden = load_golden("lighting_reference.npz")
+    got = lighting_session.earth_visibility_fraction(site["dem"], site["horizons"],
+                                                     site["earth"], **site["tile"])
+    expected = products.earth_visibility(golden["margins"], 0.0)
+    # Margins agree with the reference CPU backend within 1e-4 deg; a step
+    # can flip only where its margin lies within that of the threshold.
+    flips = np.count_nonzero(np.abs(golden["margins"]) <= MARGIN_TOL, axis=0)
+    assert np.all(np.abs(got - expected) * len(golden["margins"]) <= flips + 1e-3)

@@ -50,25 +50,34 @@ class SunLossProblem:
 
         if traversal not in TRAVERSALS:
             raise ValueError(f"traversal must be one of {sorted(TRAVERSALS)}")
-        if not tiles or len(tiles) > 32:
-            raise ValueError("1 to 32 tiles")
         self.session = session
-        self.device_dems = [session.upload_dem_grid(dem) for dem in dems]
-        self.shapes = [(dem.height, dem.width) for dem in dems]
-        self.tiles = [SiteTile(tuple(self.device_dems), int(tx), int(ty),
-                               float(maximum_distance_m), float(observer_elevation_m))
-                      for tx, ty in tiles]
+        self.maximum_distance_m = float(maximum_distance_m)
+        self.observer_elevation_m = float(observer_elevation_m)
         self.azimuth_count = int(azimuth_count)
         self.traversal = traversal
         self.disk_radius_deg = float(disk_radius_deg)
-        w = torch.as_tensor(np.asarray(weights, dtype=np.float32))
-        if w.numel() != len(tiles) * PLANE:
-            raise ValueError("weights must hold tile_count x 128 x 128 values")
-        self.weights = w.reshape(len(tiles), PLANE).contiguous().cuda()
+        self.device_dems = [session.upload_dem_grid(dem) for dem in dems]
+        self.shapes = [(dem.height, dem.width) for dem in dems]
         self.vectors = DeviceVectors(session.context,
                                      np.ascontiguousarray(sun_vectors, dtype=np.float32))
         self.time_count = self.vectors.count
         self.last_seconds = {}
+        self.use_tiles(tiles, weights)
+
+    def use_tiles(self, tiles: Sequence[tuple[int, int]], weights) -> None:
+        """Replace the tile set (1 to 32 (tile_x, tile_y) origins) and its
+        [tiles, 128, 128] pixel weights; DEMs and vectors stay resident."""
+        import torch
+
+        if not tiles or len(tiles) > 32:
+            raise ValueError("1 to 32 tiles")
+        w = torch.as_tensor(np.asarray(weights, dtype=np.float32))
+        if w.numel() != len(tiles) * PLANE:
+            raise ValueError("weights must hold tile_count x 128 x 128 values")
+        self.tiles = [SiteTile(tuple(self.device_dems), int(tx), int(ty),
+                               self.maximum_distance_m, self.observer_elevation_m)
+                      for tx, ty in tiles]
+        self.weights = w.reshape(len(tiles), PLANE).contiguous().cuda()
 
     def close(self) -> None:
         self.vectors.close()
@@ -148,6 +157,76 @@ class SunLossProblem:
         return _SunLoss.apply(self, *heights)
 
 
+class StreamedSunLoss:
+    """The loss of ``SunLossProblem`` over any number of tiles, evaluated in
+    batches of ``batch_tiles``: each batch's forward pass is followed at once
+    by its backward pass, so the argmax checkpoints of one batch only are
+    resident (about 0.4 GB per tile at 1440 azimuths) however many tiles the
+    loss covers.  The loss is a sum over tiles, so batch losses and
+    gradients add up to the whole; ``loss`` returns it as an autograd scalar
+    whose backward scales the gradient accumulated by the forward pass."""
+
+    def __init__(self, session, dems: Sequence, tiles: Sequence[tuple[int, int]], weights,
+                 sun_vectors, *, batch_tiles: int = 8, **options):
+        if not 1 <= int(batch_tiles) <= 32:
+            raise ValueError("batch_tiles must be between 1 and 32")
+        self.tiles = [(int(tx), int(ty)) for tx, ty in tiles]
+        if not self.tiles:
+            raise ValueError("at least one tile")
+        self.weights = np.asarray(weights, dtype=np.float32).reshape(len(self.tiles), PLANE)
+        self.batch_tiles = int(batch_tiles)
+        self.problem = SunLossProblem(session, dems, self.tiles[:self.batch_tiles],
+                                      self.weights[:self.batch_tiles], sun_vectors, **options)
+        self.last_seconds = {}
+
+    def close(self) -> None:
+        self.problem.close()
+
+    def value_and_gradient(self, heights=None, grad_output: float = 1.0):
+        """(loss, float64 gradients of grad_output x loss, one per DEM)."""
+        import torch
+
+        if heights is not None:
+            self.problem.set_heights(heights)
+        grads = [torch.zeros(shape, dtype=torch.float64, device="cuda")
+                 for shape in self.problem.shapes]
+        total = 0.0
+        seconds = {"forward_march": 0.0, "forward_lighting": 0.0, "backward": 0.0}
+        for start in range(0, len(self.tiles), self.batch_tiles):
+            stop = start + self.batch_tiles
+            self.problem.use_tiles(self.tiles[start:stop], self.weights[start:stop])
+            total += self.problem.forward_value()
+            for g, batch in zip(grads, self.problem.backward_value(grad_output)):
+                g += batch
+            for key in seconds:
+                seconds[key] += self.problem.last_seconds[key]
+        self.last_seconds = seconds
+        return total, grads
+
+    def loss(self, *heights):
+        """Differentiable loss (a float64 scalar tensor) of the height tensors."""
+        return _StreamedLoss.apply(self, *heights)
+
+
+def psr_boundary_weights(psr, resolution_m: float, distance_m: float = 500.0) -> np.ndarray:
+    """float32 weights, 1 on pixels within ``distance_m`` of the boundary of a
+    PSR mask (pixels whose 4-neighbourhood holds both classes) and 0
+    elsewhere: the region whose sun fraction the large sensitivity run
+    differentiates.  Host preparation (scipy's Euclidean distance transform)."""
+    from scipy import ndimage
+
+    mask = np.asarray(psr) != 0
+    boundary = np.zeros_like(mask)
+    boundary[:-1, :] |= mask[:-1, :] != mask[1:, :]
+    boundary[1:, :] |= mask[1:, :] != mask[:-1, :]
+    boundary[:, :-1] |= mask[:, :-1] != mask[:, 1:]
+    boundary[:, 1:] |= mask[:, 1:] != mask[:, :-1]
+    if not boundary.any():
+        return np.zeros(mask.shape, dtype=np.float32)
+    distance = ndimage.distance_transform_edt(~boundary) * float(resolution_m)
+    return (distance <= float(distance_m)).astype(np.float32)
+
+
 def _function():
     import torch
 
@@ -164,16 +243,32 @@ def _function():
             grads = ctx.problem.backward_value(float(grad_output))
             return (None, *[g.to(dtype) for g, dtype in zip(grads, ctx.dtypes)])
 
-    return SunLoss
+    class StreamedLoss(torch.autograd.Function):
+        @staticmethod
+        def forward(ctx, streamed, *heights):
+            ctx.dtypes = [h.dtype for h in heights]
+            value, ctx.grads = streamed.value_and_gradient(heights)
+            return torch.tensor(value, dtype=torch.float64, device=heights[0].device)
+
+        @staticmethod
+        def backward(ctx, grad_output):
+            scale = grad_output.to(torch.float64)
+            return (None, *[(scale * g).to(dtype) for g, dtype in zip(ctx.grads, ctx.dtypes)])
+
+    return SunLoss, StreamedLoss
 
 
-class _SunLossProxy:
-    _cls = None
+class _FunctionProxy:
+    _classes = None
+
+    def __init__(self, which: int):
+        self.which = which
 
     def apply(self, *args):
-        if _SunLossProxy._cls is None:
-            _SunLossProxy._cls = _function()
-        return _SunLossProxy._cls.apply(*args)
+        if _FunctionProxy._classes is None:
+            _FunctionProxy._classes = _function()
+        return _FunctionProxy._classes[self.which].apply(*args)
 
 
-_SunLoss = _SunLossProxy()
+_SunLoss = _FunctionProxy(0)
+_StreamedLoss = _FunctionProxy(1)

@@ -190,3 +190,40 @@ def test_adjoint_rejects_inconsistent_problems(problem, cuda_session):
     with pytest.raises(ValueError):
         p.backward_value.__self__.set_heights([heights, heights])
     assert torch.isfinite(heights).all()
+
+
+def test_streamed_batches_add_up_to_the_one_shot_loss_and_gradient(cuda_session):
+    import torch
+
+    from lunarscout_b200.adjoint import StreamedSunLoss, SunLossProblem
+    from lunarscout_b200.synthetic import SyntheticDemSpec, hours_between, sun_vectors, \
+        synthetic_dem
+
+    dem = synthetic_dem(SyntheticDemSpec(512, 10.0, craters=30, crater_max_m=1500.0, seed=23))
+    tiles = [(128, 128), (256, 128), (128, 256), (256, 256), (384, 384)]
+    weights = np.random.default_rng(24).uniform(0.0, 1.0, (len(tiles), 128, 128))
+    vectors = sun_vectors(hours_between("2030-03-01T00", "2030-03-03T00", 4.0))
+    options = dict(maximum_distance_m=5_000.0, observer_elevation_m=OBSERVER, azimuth_count=AZ)
+    heights = torch.from_numpy(dem.elevation_m).cuda()
+    whole = SunLossProblem(cuda_session, [dem], tiles, weights, vectors, **options)
+    streamed = StreamedSunLoss(cuda_session, [dem], tiles, weights, vectors, batch_tiles=2,
+                               **options)
+    try:
+        loss = whole.forward_value([heights])
+        (grad,) = whole.backward_value(1.0)
+        value, (streamed_grad,) = streamed.value_and_gradient([heights])
+        assert loss > 0.0
+        assert abs(value - loss) <= 1e-12 * abs(loss)
+        grad, streamed_grad = grad.cpu().numpy(), streamed_grad.cpu().numpy()
+        scale = np.abs(grad).max()
+        assert scale > 0.0
+        assert np.abs(streamed_grad - grad).max() <= 1e-12 * scale
+        h = heights.clone().requires_grad_(True)
+        out = streamed.loss(h)
+        (2.5 * out).backward()
+        assert abs(float(out) - value) <= 1e-12 * abs(value)
+        np.testing.assert_allclose(h.grad.cpu().numpy(), (2.5 * streamed_grad).astype(np.float32),
+                                   rtol=1e-6, atol=1e-6 * 2.5 * scale)
+    finally:
+        whole.close()
+        streamed.close()

@@ -799,6 +799,109 @@ def adjoint_benchmark(session, args, rank):
     return result
 
 
+SENSITIVITY_SIDE = 8192
+SENSITIVITY_BATCH = 4
+SENSITIVITY_STEPS = 26281  # 3 years at 1 h
+
+
+def sensitivity_benchmark(session, regional, args, rank):
+    """A slice of the large batched sensitivity run: an 8192 x 8192 primary
+    at 5 m (the site recipe, 2400 craters) with the regional DEM, 8 tiles
+    around the centre, 200 km rays, 3 years of hourly Sun vectors.
+    Horizons by the persistent ladder march, PSR over all 26,281 vectors,
+    weights 1 within 500 m of each tile's PSR boundary, then the streamed
+    adjoint of the weighted mean smooth sun fraction in batches of 4 tiles
+    (the argmax checkpoints of one batch resident at a time)."""
+    import ctypes
+
+    import torch
+
+    from lunarscout_b200 import _native, synthetic
+    from lunarscout_b200.adjoint import StreamedSunLoss, psr_boundary_weights
+    from lunarscout_b200.contract import projection_array
+    from lunarscout_b200.cuda_backend import SiteTile
+    from lunarscout_b200.lightmap_cuda import DeviceVectors
+
+    started = time.perf_counter()
+    primary = synthetic.site_dem(SENSITIVITY_SIDE, 5.0, craters=2400, seed=5)
+    build_s = time.perf_counter() - started
+    centre = SENSITIVITY_SIDE // 2
+    tiles = [(centre + dx * TILE, centre + dy * TILE) for dy in (-1, 0) for dx in (-2, -1, 0, 1)]
+    count = len(tiles)
+    plane = TILE * TILE
+    vectors = synthetic.sun_vectors(np.arange(SENSITIVITY_STEPS, dtype=np.float64))
+    dems = [session.upload_dem_grid(primary), session.upload_dem_grid(regional)]
+    horizons = torch.empty((count, plane, AZIMUTHS), dtype=torch.float32, device="cuda")
+    site_tiles = [SiteTile(tuple(dems), tx, ty, RANGE_M, OBSERVER_M) for tx, ty in tiles]
+    session.march_sites(site_tiles, device_out=horizons.data_ptr(), traversal="ladder",
+                        degrees=True)
+    _, march_s = session.march_sites(site_tiles, device_out=horizons.data_ptr(),
+                                     traversal="ladder", degrees=True)
+    patches = torch.stack([torch.from_numpy(np.ascontiguousarray(
+        primary.elevation_m[ty:ty + TILE, tx:tx + TILE])) for tx, ty in tiles]).cuda()
+    geo = np.ascontiguousarray(np.repeat(primary.geo_transform[None, :], count, 0))
+    proj = np.ascontiguousarray(np.repeat(projection_array(primary.projection)[None, :],
+                                          count, 0))
+    windows = np.array([(tx, ty, TILE, TILE) for tx, ty in tiles], dtype=np.int32)
+    table = DeviceVectors(session.context, vectors.astype(np.float32))
+    frames = torch.empty(count * plane * 12, dtype=torch.float32, device="cuda")
+    psr = torch.empty((count, plane), dtype=torch.uint8, device="cuda")
+    lib = _native.library()
+
+    def psr_launch():
+        _native.check(lib.ls200_lighting_device(
+            session.context, count, ctypes.c_void_p(patches.data_ptr()), geo.ctypes.data,
+            proj.ctypes.data, windows.ctypes.data, ctypes.c_void_p(horizons.data_ptr()),
+            table.handle, 0, SENSITIVITY_STEPS, 3, ctypes.c_void_p(frames.data_ptr()),
+            ctypes.c_void_p(psr.data_ptr())))
+
+    psr_launch()
+    torch.cuda.synchronize()
+    begin, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    begin.record()
+    psr_launch()
+    end.record()
+    torch.cuda.synchronize()
+    psr_s = begin.elapsed_time(end) / 1000.0
+    table.close()
+    masks = psr.cpu().numpy().reshape(count, TILE, TILE)
+    weights = np.stack([psr_boundary_weights(m, 5.0, 500.0) for m in masks])
+    del horizons
+    for dem in dems:
+        dem.close()
+    streamed = StreamedSunLoss(session, [primary, regional], tiles, weights, vectors,
+                               batch_tiles=SENSITIVITY_BATCH, maximum_distance_m=RANGE_M,
+                               observer_elevation_m=OBSERVER_M, azimuth_count=AZIMUTHS,
+                               traversal="ladder")
+    heights = [torch.from_numpy(primary.elevation_m).cuda(),
+               torch.from_numpy(regional.elevation_m).cuda()]
+    try:
+        loss, grads = streamed.value_and_gradient(heights)
+        seconds = dict(streamed.last_seconds)
+        free, total = torch.cuda.mem_get_info()
+        nonzero = int(torch.count_nonzero(grads[0]))
+    finally:
+        streamed.close()
+    forward_s = seconds["forward_march"] + seconds["forward_lighting"]
+    rays = count * plane * AZIMUTHS
+    return {
+        "workload": "8 tiles of an 8192x8192 5 m primary + 240 m regional, 200 km rays, "
+                    "3 years hourly (26,281 Sun vectors)",
+        "tiles": count, "batch_tiles": SENSITIVITY_BATCH, "time_steps": SENSITIVITY_STEPS,
+        "dem_build_s": build_s,
+        "march_rays_per_s": rays / march_s,
+        "psr_px_steps_per_s": count * plane * SENSITIVITY_STEPS / psr_s,
+        "psr_fraction": float((masks > 0).mean()),
+        "weighted_fraction": float(weights.mean()),
+        "loss": loss, "forward_s": forward_s, "backward_s": seconds["backward"],
+        "adjoint_over_forward": seconds["backward"] / forward_s,
+        "gradient_nonzero_cells": nonzero,
+        "device_memory_in_use_gb": (total - free) / 1e9,
+        "memory_note": "cudaMemGetInfo after the run; the library keeps its largest buffers, "
+                       "so this includes the run's peak",
+    }
+
+
 def run_ours(args):
     import torch
     import torch.distributed as dist
@@ -922,6 +1025,8 @@ def run_ours(args):
     multisite = None if args.skip_multisite else multisite_benchmark(session, stream, args,
                                                                      world, rank)
     adjoint = None if args.skip_adjoint else adjoint_benchmark(session, args, rank)
+    sensitivity = (None if args.skip_sensitivity or world > 1
+                   else sensitivity_benchmark(session, regional, args, rank))
     # The public generator runs on device 0 (as the reference's does): 1 GPU only.
     generate = (None if args.skip_generate or world > 1
                 else generate_benchmark(primary, regional, rank))
@@ -975,6 +1080,7 @@ def run_ours(args):
             "multisite": multisite,
             "adjoint": adjoint,
             "generate_horizons": generate,
+            "sensitivity": sensitivity,
         }
         print(json.dumps(line), flush=True)
     session.close()
@@ -1082,6 +1188,8 @@ def main():
                         help="leave out the DEM-adjoint (differentiable lighting) leg")
     parser.add_argument("--skip-generate", action="store_true",
                         help="leave out the end-to-end tile-generator leg")
+    parser.add_argument("--skip-sensitivity", action="store_true",
+                        help="leave out the 8192^2 streamed-adjoint sensitivity slice")
     parser.add_argument("--profile", nargs="?", const="site", choices=("site", "multisite"),
                         help="small profiling case, no timing: 'site' = one site-scale tile "
                              "(two march steps, two lighting launches); 'multisite' = four "

@@ -1,0 +1,132 @@
+"""The fused horizon -> lighting chain on the B200: its tiles are the
+generator's bytes, and each product equals the per-patch session call fed
+the same horizons (host round trip) — the chain only removes the round trip."""
+
+from __future__ import annotations
+
+from datetime import datetime, timedelta, timezone
+
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def chain_case():
+    from lunarscout_b200 import synthetic
+    from lunarscout_b200.chain import ProductChain
+    from lunarscout_b200.pipeline import enumerate_patches
+    from lunarscout_b200.synthetic import SyntheticDemSpec, synthetic_dem
+
+    dem = synthetic_dem(SyntheticDemSpec(320, 20.0, craters=30, seed=5))
+    small = type(dem)(np.ascontiguousarray(dem.elevation_m[:200, :300]), dem.geo_transform,
+                      dem.projection)
+    chain = ProductChain([small], maximum_distance_m=40_000.0, observer_elevation_m=0.5)
+    patches = enumerate_patches(small.width, small.height)
+    batch = chain.march(patches)
+    hours = synthetic.hours_between("2029-01-25T00", "2029-03-05T00", 6.0)
+    yield dict(chain=chain, dem=small, patches=patches, batch=batch, hours=hours,
+               sun=synthetic.sun_vectors(hours), earth=synthetic.earth_vectors(hours))
+    chain.close()
+
+
+def _host(batch, i):
+    """The horizons a .cbin round trip would hand the sessions at -inf (-50),
+    unquantized."""
+    h = batch.horizons[i].view(128, 128, 1440).cpu().numpy()
+    return np.where(np.isneginf(h), np.float32(-50.0), h)
+
+
+def _tile(patch):
+    return dict(tile_y=patch.tile_y, tile_x=patch.tile_x, valid_height=patch.height,
+                valid_width=patch.width)
+
+
+@pytest.mark.parametrize("compress", [False, True])
+def test_chain_tiles_are_the_generator_bytes(tmp_path, chain_case, compress):
+    from lunarscout_b200.file_format import HorizonTileStore, TileCodec
+    from lunarscout_b200.horizon import generate_horizons_from_grids
+
+    chain, batch = chain_case["chain"], chain_case["batch"]
+    assert len(batch) == 6 and any(p.width < 128 or p.height < 128 for p in batch.patches)
+    generate_horizons_from_grids(tmp_path / "generator", [chain_case["dem"]],
+                                 observer_height_m=0.5, compress=compress,
+                                 maximum_distance_m=40_000.0)
+    codec = TileCodec(context=chain.session.context)
+    try:
+        store = HorizonTileStore(tmp_path / "chain", codec=codec)
+        chain.write_tiles(batch, store, compress=compress)
+        chain.wait_for_writes()
+    finally:
+        codec.close()
+    written = sorted((tmp_path / "generator").rglob("horizon_*"))
+    assert len(written) == 6
+    for path in written:
+        twin = tmp_path / "chain" / path.relative_to(tmp_path / "generator")
+        assert twin.read_bytes() == path.read_bytes(), path.name
+
+
+def test_chain_products_equal_the_per_patch_sessions(chain_case):
+    from lunarscout_b200.lightmap_cuda import LightmapCudaSession
+    from lunarscout_b200.psr_cuda import PsrCudaSession
+    from lunarscout_b200.safe_haven import month_bands, month_indices
+
+    chain, batch, dem = chain_case["chain"], chain_case["batch"], chain_case["dem"]
+    sun, earth, hours = chain_case["sun"], chain_case["earth"], chain_case["hours"]
+    lighting = LightmapCudaSession(time_batch_size=32)
+    psr_session = PsrCudaSession()
+    start = datetime(2029, 1, 25, tzinfo=timezone.utc)
+    times = [start + timedelta(hours=float(h)) for h in hours]
+    bands = month_bands(times)
+    months = month_indices(times, bands)
+    sample_hours = np.full(len(hours), 6.0)
+    windows = np.array([[0, 40], [40, 100], [100, len(hours)]], dtype=np.int32)
+    try:
+        fractions = chain.sun_fractions(batch, sun).cpu().numpy()
+        encoded = chain.sun_fraction_bytes(batch, sun).cpu().numpy()
+        psr = chain.psr(batch, sun)
+        missions = chain.mission_durations(batch, sun, sample_hours=sample_hours,
+                                           start_windows=windows, earth_vectors_m=earth)
+        havens = chain.safe_haven(batch, sun, earth, month_index_of=months,
+                                  band_count=len(bands), time_step_hours=6.0,
+                                  sunlight_threshold=0.5, earth_threshold_deg=1.0)
+        visible = chain.earth_visibility(batch, earth)
+        for i, patch in enumerate(batch.patches):
+            horizons, tile = _host(batch, i), _tile(patch)
+            h, w = patch.height, patch.width
+            expected = np.stack(list(lighting.iter_patch_fraction_tiles(dem, horizons, sun,
+                                                                        **tile)))
+            got = fractions[i].reshape(len(sun), 128, 128)[:, :h, :w]
+            np.testing.assert_array_equal(got, expected)
+            expected = np.stack(list(lighting.iter_patch_tiles(dem, horizons, sun, **tile)))
+            np.testing.assert_array_equal(encoded[i].reshape(len(sun), 128, 128)[:, :h, :w],
+                                          expected)
+            np.testing.assert_array_equal(psr[i], psr_session.compute_patch(dem, horizons,
+                                                                            sun, **tile))
+            np.testing.assert_array_equal(missions[i], lighting.mission_durations(
+                dem, horizons, sun, sample_hours=sample_hours, start_windows=windows,
+                earth_vectors_m=earth, **tile))
+            np.testing.assert_array_equal(havens[i], np.stack(
+                lighting.safe_haven_durations(dem, horizons, sun, earth, month_index_of=months,
+                                              band_count=len(bands), time_step_hours=6.0,
+                                              sunlight_threshold=0.5, earth_threshold_deg=1.0,
+                                              **tile)))
+            np.testing.assert_array_equal(visible[i], lighting.earth_visibility_fraction(
+                dem, horizons, earth, **tile))
+        assert any(float(m.max()) > 0.0 for m in missions)
+    finally:
+        lighting.close()
+        psr_session.close()
+
+
+def test_chain_validation(chain_case):
+    from lunarscout_b200.chain import ProductChain
+
+    chain = chain_case["chain"]
+    with pytest.raises(ValueError):
+        chain.march([])
+    with pytest.raises(ValueError):
+        chain.march(list(chain_case["patches"]) * 6)
+    with pytest.raises(ValueError):
+        ProductChain([chain_case["dem"]], traversal="sideways")

@@ -99,6 +99,11 @@ __global__ void __launch_bounds__(128) frames_kernel(const __grid_constant__ Lig
     for (int k = 0; k < 12; ++k) dst[k] = f.v[k];
 }
 
+// Per-thread window of staged horizon bins (stride 33 spreads the threads'
+// windows over the 32 shared-memory banks).
+constexpr int kWindowBins = 32;
+constexpr int kWindowStride = kWindowBins + 1;
+
 template <int kSignal>
 __global__ void __launch_bounds__(128) lighting_kernel(const __grid_constant__ LightingBatch B) {
     const int tile = blockIdx.z;
@@ -106,12 +111,14 @@ __global__ void __launch_bounds__(128) lighting_kernel(const __grid_constant__ L
     if (index >= kPatch * kPatch) return;
     const TileGeo &g = B.tiles[tile];
     const int sample = index % kPatch, line = index / kPatch;
-    const int t0 = B.time_start + blockIdx.y * B.chunk;
-    const int t1 = min(t0 + B.chunk, B.time_start + B.time_count);
+    // Chunk blockIdx.y covers positions [k0, k1) of the launch's order.
+    const int k0 = blockIdx.y * B.chunk;
+    const int k1 = min(k0 + B.chunk, B.time_count);
     const size_t plane = static_cast<size_t>(kPatch) * kPatch;
     const size_t tile_out = static_cast<size_t>(tile) * B.time_count * plane;
     if (sample >= g.valid_width || line >= g.valid_height) {
-        for (int t = t0; t < t1; ++t) {
+        for (int k = k0; k < k1; ++k) {
+            const int t = B.order ? __ldg(B.order + k) : B.time_start + k;
             const size_t o = tile_out + static_cast<size_t>(t - B.time_start) * plane + index;
             if (kSignal == kSignalBytes) static_cast<uint8_t *>(B.out)[o] = 0;
             else static_cast<float *>(B.out)[o] = 0.0f;
@@ -123,15 +130,59 @@ __global__ void __launch_bounds__(128) lighting_kernel(const __grid_constant__ L
 #pragma unroll
     for (int k = 0; k < 12; ++k) f.v[k] = src[k];
     const float *horizon = B.horizons + (static_cast<size_t>(tile) * plane + index) * kAzimuths;
-    for (int t = t0; t < t1; ++t) {
+    // Stage the bins this chunk reads.  In longitude order the body's
+    // azimuth moves monotonically across a chunk, so the bins between those
+    // of its first and last steps (plus the signal's span and a margin of 2
+    // on each side) cover it; a step outside them reads its row directly.
+    __shared__ float windows[128 * kWindowStride];
+    float *window = windows + threadIdx.x * kWindowStride;
+    constexpr int kSpan = kSignal == kSignalMargin ? 2 : 5;
+    int first = 0, width = 0;
+    if (B.order && k1 > k0) {
+        float azimuth_deg, elevation;
+        const float *v = B.vectors + 3 * static_cast<size_t>(__ldg(B.order + k0));
+        body_direction(f, __ldg(v), __ldg(v + 1), __ldg(v + 2), azimuth_deg, elevation);
+        const int a = kSignal == kSignalMargin ? margin_position(azimuth_deg).left
+                                               : sun_position(azimuth_deg).left;
+        v = B.vectors + 3 * static_cast<size_t>(__ldg(B.order + k1 - 1));
+        body_direction(f, __ldg(v), __ldg(v + 1), __ldg(v + 2), azimuth_deg, elevation);
+        const int b = kSignal == kSignalMargin ? margin_position(azimuth_deg).left
+                                               : sun_position(azimuth_deg).left;
+        int arc = b - a;
+        if (arc < 0) arc += kAzimuths;
+        int start = arc <= kAzimuths / 2 ? a : b;
+        if (arc > kAzimuths / 2) arc = kAzimuths - arc;
+        start -= 2;
+        if (start < 0) start += kAzimuths;
+        if (arc + kSpan + 4 <= kWindowBins) {
+            first = start;
+            width = arc + kSpan + 4;
+            for (int i = 0; i < width; ++i) {
+                int bin = first + i;
+                if (bin >= kAzimuths) bin -= kAzimuths;
+                window[i] = __ldg(horizon + bin);
+            }
+        }
+    }
+    for (int k = k0; k < k1; ++k) {
+        const int t = B.order ? __ldg(B.order + k) : B.time_start + k;
         const float *v = B.vectors + 3 * static_cast<size_t>(t);
         float azimuth_deg, elevation;
         body_direction(f, __ldg(v), __ldg(v + 1), __ldg(v + 2), azimuth_deg, elevation);
         const size_t o = tile_out + static_cast<size_t>(t - B.time_start) * plane + index;
+        const BinPosition p = kSignal == kSignalMargin ? margin_position(azimuth_deg)
+                                                       : sun_position(azimuth_deg);
+        int offset = p.left - first;
+        if (offset < 0) offset += kAzimuths;
+        const bool staged = offset + kSpan <= width;
         if (kSignal == kSignalMargin) {
-            static_cast<float *>(B.out)[o] = horizon_margin(horizon, azimuth_deg, elevation);
+            static_cast<float *>(B.out)[o] =
+                staged ? horizon_margin_bins(SharedBins{window, offset}, p.fraction, elevation)
+                       : horizon_margin_bins(GlobalBins{horizon, p.left}, p.fraction, elevation);
         } else {
-            const float visible = sun_fraction(horizon, azimuth_deg, elevation);
+            const float visible =
+                staged ? sun_fraction_bins(SharedBins{window, offset}, p.fraction, elevation)
+                       : sun_fraction_bins(GlobalBins{horizon, p.left}, p.fraction, elevation);
             if (kSignal == kSignalBytes)
                 static_cast<uint8_t *>(B.out)[o] =
                     static_cast<uint8_t>(static_cast<int>(__fmul_rn(255.0f, visible)));
@@ -200,8 +251,52 @@ int lighting_chunk(ls200_context *ctx, int tiles, int time_count) {
     return (time_count + chunks - 1) / chunks;
 }
 
-void lighting_launch(ls200_context *ctx, LightingBatch &B, int tiles, int signal) {
+// window = the entries of `order` inside [t0, t0 + n), in order: one block,
+// each thread counting and then copying a contiguous run of `order` at the
+// offset given by a block scan of the counts.
+constexpr int kOrderThreads = 1024;
+
+__global__ void __launch_bounds__(kOrderThreads) order_window_kernel(
+    const int *__restrict__ order, int count, int t0, int n, int *__restrict__ window) {
+    __shared__ int sums[kOrderThreads];
+    const int per = (count + kOrderThreads - 1) / kOrderThreads;
+    const int begin = min(count, static_cast<int>(threadIdx.x) * per);
+    const int end = min(count, begin + per);
+    int mine = 0;
+    for (int k = begin; k < end; ++k) {
+        const int t = order[k];
+        mine += (t >= t0 && t < t0 + n) ? 1 : 0;
+    }
+    sums[threadIdx.x] = mine;
+    __syncthreads();
+    for (int offset = 1; offset < kOrderThreads; offset <<= 1) {
+        const int add = threadIdx.x >= static_cast<unsigned>(offset) ? sums[threadIdx.x - offset]
+                                                                     : 0;
+        __syncthreads();
+        sums[threadIdx.x] += add;
+        __syncthreads();
+    }
+    int position = sums[threadIdx.x] - mine;
+    for (int k = begin; k < end; ++k) {
+        const int t = order[k];
+        if (t >= t0 && t < t0 + n) window[position++] = t;
+    }
+}
+
+void lighting_launch(ls200_context *ctx, LightingBatch &B, int tiles, int signal,
+                     const ls200_vectors *table) {
     ensure_lighting_constants(ctx);
+    B.order = nullptr;
+    if (table && table->order && signal != kSignalPsr) {
+        if (B.time_start == 0 && B.time_count == table->count) {
+            B.order = table->order;
+        } else {
+            order_window_kernel<<<1, kOrderThreads, 0, ctx->stream>>>(
+                table->order, table->count, B.time_start, B.time_count, table->window);
+            LS_CUDA(cudaGetLastError());
+            B.order = table->window;
+        }
+    }
     dim3 grid_frames(kPatch * kPatch / 128, tiles);
     frames_kernel<<<grid_frames, 128, 0, ctx->stream>>>(B);
     LS_CUDA(cudaGetLastError());
@@ -210,6 +305,11 @@ void lighting_launch(ls200_context *ctx, LightingBatch &B, int tiles, int signal
         psr_kernel<<<grid, 128, 0, ctx->stream>>>(B);
     } else {
         B.chunk = lighting_chunk(ctx, tiles, B.time_count);
+        // In longitude order a chunk of c steps sweeps about c * 1440 / T
+        // bins; keep that to 20 so the chunk's bins fit the staged window.
+        if (B.order)
+            B.chunk = std::min(B.chunk,
+                               std::max(16, (kWindowBins - 12) * B.time_count / kAzimuths));
         dim3 grid(kPatch * kPatch / 128, (B.time_count + B.chunk - 1) / B.chunk, tiles);
         if (signal == kSignalFraction)
             lighting_kernel<kSignalFraction><<<grid, 128, 0, ctx->stream>>>(B);

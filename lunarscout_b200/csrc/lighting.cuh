@@ -11,6 +11,12 @@ struct ls200_vectors {
     ls200_context *ctx = nullptr;
     float *data = nullptr;  // device [count, 3]
     int count = 0;
+    // device [count]: time indices sorted by the vector's longitude
+    // atan2(y, x).  For a polar site the body's local azimuth follows its
+    // longitude, so in this order consecutive steps read neighbouring
+    // horizon bins.
+    int *order = nullptr;
+    int *window = nullptr;  // device [count]: one launch's sub-range of `order`
 };
 
 namespace ls200 {
@@ -38,9 +44,15 @@ struct LightingBatch {
     float *frames;           // [tiles, 16384, 12]
     void *out;               // [tiles, time_count, 16384] (PSR: [tiles, 16384])
     int time_start, time_count, chunk;
+    // [time_count] the launch's time indices in processing order, or NULL
+    // for time order; outputs stay in time order either way.
+    const int *order;
 };
 
-void lighting_launch(ls200_context *ctx, LightingBatch &batch, int tiles, int signal);
+// With `table` (the vector table of the launch), fraction / byte / margin
+// launches visit their time steps in the table's longitude order.
+void lighting_launch(ls200_context *ctx, LightingBatch &batch, int tiles, int signal,
+                     const ls200_vectors *table = nullptr);
 void sun_fraction_launch(ls200_context *ctx, const float *horizons, const float *azimuth_deg,
                          const float *elevation_deg, int n, float *out);
 void ensure_lighting_constants(ls200_context *ctx);
@@ -105,15 +117,49 @@ __device__ __forceinline__ void body_direction(const Frame32 &f, float vx, float
 
 // Body-centre elevation minus the horizon interpolated at its azimuth
 // (lightmap_cpu.py:121-141).
-__device__ __forceinline__ float horizon_margin(const float *horizon, float azimuth_deg,
-                                                float elevation) {
+//
+// The signals read the horizon bins left, left+1, ... (wrapped at 1440)
+// through a bin accessor: GlobalBins reads the pixel's row, SharedBins a
+// window of it staged in shared memory.  Both return the same values.
+struct GlobalBins {
+    const float *horizon;
+    int left;
+    __device__ __forceinline__ float operator()(int k) const {
+        int b = left + k;
+        if (b >= kAzimuths) b -= kAzimuths;
+        return __ldg(horizon + b);
+    }
+};
+struct SharedBins {
+    const float *window;
+    int offset;  // position of bin `left` in the window
+    __device__ __forceinline__ float operator()(int k) const { return window[offset + k]; }
+};
+
+// First bin and interpolation fraction of the margin (2 bins).
+struct BinPosition {
+    int left;
+    float fraction;
+};
+__device__ __forceinline__ BinPosition margin_position(float azimuth_deg) {
     const float position = __fmul_rn(azimuth_deg, 4.0f);
     int left = static_cast<int>(position);
     const float fraction = __fsub_rn(position, static_cast<float>(left));
     if (left >= kAzimuths) left -= kAzimuths;
-    const int right = left + 1 >= kAzimuths ? 0 : left + 1;
-    const float hl = __ldg(horizon + left), hr = __ldg(horizon + right);
+    return BinPosition{left, fraction};
+}
+
+template <class Bins>
+__device__ __forceinline__ float horizon_margin_bins(const Bins &bin, float fraction,
+                                                     float elevation) {
+    const float hl = bin(0), hr = bin(1);
     return __fsub_rn(elevation, __fadd_rn(hl, __fmul_rn(fraction, __fsub_rn(hr, hl))));
+}
+
+__device__ __forceinline__ float horizon_margin(const float *horizon, float azimuth_deg,
+                                                float elevation) {
+    const BinPosition p = margin_position(azimuth_deg);
+    return horizon_margin_bins(GlobalBins{horizon, p.left}, p.fraction, elevation);
 }
 
 // Visible fraction of the solar disk: 16 vertical slices of a 0.27-deg disk
@@ -127,21 +173,25 @@ __device__ __forceinline__ float horizon_margin(const float *horizon, float azim
 // float32 rounding of degrees), every slice is fully lit (the float32 sum of
 // the 2c_k is then exactly the normaliser: fraction 1) or fully dark
 // (fraction 0), and the loop is skipped.
-__device__ __forceinline__ float sun_fraction(const float *horizon, float azimuth_deg,
-                                              float elevation) {
+// First bin and fraction of the disk's first slice (the slices then read
+// bins left .. left+4: 16 steps of 0.135 bin from a fraction below 1).
+__device__ __forceinline__ BinPosition sun_position(float azimuth_deg) {
     const float left_position = __fmul_rn(__fsub_rn(__fsub_rn(azimuth_deg, 0.27f), 0.125f), 4.0f);
     int left = static_cast<int>(left_position);
-    float fraction = __fsub_rn(left_position, static_cast<float>(left));
+    const float fraction = __fsub_rn(left_position, static_cast<float>(left));
     if (left < 0) left += kAzimuths;
     else if (left >= kAzimuths) left -= kAzimuths;
-    int right = left + 1 >= kAzimuths ? 0 : left + 1;
+    return BinPosition{left, fraction};
+}
+
+template <class Bins>
+__device__ __forceinline__ float sun_fraction_bins(const Bins &bin, float fraction,
+                                                   float elevation) {
     {
-        float lo = __ldg(horizon + left), hi = lo;
+        float lo = bin(0), hi = lo;
 #pragma unroll
         for (int k = 1; k <= 4; ++k) {
-            int b = left + k;
-            if (b >= kAzimuths) b -= kAzimuths;
-            const float h = __ldg(horizon + b);
+            const float h = bin(k);
             lo = fminf(lo, h);
             hi = fmaxf(hi, h);
         }
@@ -150,8 +200,9 @@ __device__ __forceinline__ float sun_fraction(const float *horizon, float azimut
         if (hi + span <= elevation - cmax - 1e-3f) return 1.0f;
         if (lo - span >= elevation + cmax + 1e-3f) return 0.0f;
     }
-    float left_elevation = __ldg(horizon + left);
-    float right_elevation = __ldg(horizon + right);
+    int right = 1;
+    float left_elevation = bin(0);
+    float right_elevation = bin(1);
     float delta = __fsub_rn(right_elevation, left_elevation);
     float photons = 0.0f;
 #pragma unroll
@@ -167,14 +218,20 @@ __device__ __forceinline__ float sun_fraction(const float *horizon, float azimut
         }
         fraction = __fadd_rn(fraction, 0.135f);
         if (fraction >= 1.0f) {
-            right = right + 1 >= kAzimuths ? 0 : right + 1;
+            ++right;
             left_elevation = right_elevation;
-            right_elevation = __ldg(horizon + right);
+            right_elevation = bin(right);
             delta = __fsub_rn(right_elevation, left_elevation);
             fraction = __fsub_rn(fraction, 1.0f);
         }
     }
     return __fdiv_rn(photons, c_max_photons);
+}
+
+__device__ __forceinline__ float sun_fraction(const float *horizon, float azimuth_deg,
+                                              float elevation) {
+    const BinPosition p = sun_position(azimuth_deg);
+    return sun_fraction_bins(GlobalBins{horizon, p.left}, p.fraction, elevation);
 }
 #endif
 

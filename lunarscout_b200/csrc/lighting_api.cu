@@ -1,7 +1,9 @@
 // C-ABI entry points of the lighting products.
 #include "lighting.cuh"
 
+#include <algorithm>
 #include <cmath>
+#include <numeric>
 #include <vector>
 
 namespace ls200 {
@@ -25,6 +27,8 @@ void release_lighting_state(ls200_context *ctx) {
     if (!ctx->lighting) return;
     for (ls200_vectors *v : ctx->lighting->vectors) {
         cudaFree(v->data);
+        cudaFree(v->order);
+        cudaFree(v->window);
         delete v;
     }
     delete ctx->lighting;
@@ -60,20 +64,41 @@ ls200_status ls200_vectors_create(ls200_context *ctx, const float *vectors, int 
         LS_REQUIRE(count > 0, "at least one vector is required");
         std::lock_guard<std::mutex> hold(ctx->lock);
         activate(ctx);
+        // Time indices by longitude (ties by index); non-finite keys sort as 0.
+        std::vector<double> key(count);
+        for (int t = 0; t < count; ++t) {
+            const double k = std::atan2(static_cast<double>(vectors[3 * t + 1]),
+                                        static_cast<double>(vectors[3 * t]));
+            key[t] = std::isfinite(k) ? k : 0.0;
+        }
+        std::vector<int> order(count);
+        std::iota(order.begin(), order.end(), 0);
+        std::stable_sort(order.begin(), order.end(),
+                         [&](int a, int b) { return key[a] < key[b]; });
         auto v = new ls200_vectors();
         v->ctx = ctx;
         v->count = count;
-        cudaError_t e = cudaMalloc(&v->data, sizeof(float) * 3 * size_t(count));
-        if (e != cudaSuccess) {
+        auto release = [&] {
+            if (v->data) cudaFree(v->data);
+            if (v->order) cudaFree(v->order);
+            if (v->window) cudaFree(v->window);
             delete v;
+        };
+        cudaError_t e = cudaMalloc(&v->data, sizeof(float) * 3 * size_t(count));
+        if (e == cudaSuccess) e = cudaMalloc(&v->order, sizeof(int) * size_t(count));
+        if (e == cudaSuccess) e = cudaMalloc(&v->window, sizeof(int) * size_t(count));
+        if (e != cudaSuccess) {
+            release();
             throw Error(LS200_ERR_CUDA, std::string("cudaMalloc: ") + cudaGetErrorString(e));
         }
         e = cudaMemcpyAsync(v->data, vectors, sizeof(float) * 3 * size_t(count),
                             cudaMemcpyHostToDevice, ctx->stream);
+        if (e == cudaSuccess)
+            e = cudaMemcpyAsync(v->order, order.data(), sizeof(int) * size_t(count),
+                                cudaMemcpyHostToDevice, ctx->stream);
         if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
         if (e != cudaSuccess) {
-            cudaFree(v->data);
-            delete v;
+            release();
             throw Error(LS200_ERR_CUDA, std::string("vector upload: ") + cudaGetErrorString(e));
         }
         state_of(ctx).vectors.insert(v);
@@ -89,6 +114,8 @@ ls200_status ls200_vectors_destroy(ls200_vectors *vectors) {
         cudaStreamSynchronize(vectors->ctx->stream);
         state_of(vectors->ctx).vectors.erase(vectors);
         cudaFree(vectors->data);
+        cudaFree(vectors->order);
+        cudaFree(vectors->window);
         delete vectors;
     });
 }
@@ -198,7 +225,7 @@ ls200_status ls200_lighting_device(ls200_context *ctx, int tile_count, const flo
         B.out = out;
         B.time_start = signal == kSignalPsr ? 0 : time_start;
         B.time_count = signal == kSignalPsr ? vectors->count : time_count;
-        lighting_launch(ctx, B, tile_count, signal);
+        lighting_launch(ctx, B, tile_count, signal, vectors);
     });
 }
 

@@ -104,6 +104,48 @@ __global__ void __launch_bounds__(128) frames_kernel(const __grid_constant__ Lig
 constexpr int kWindowBins = 32;
 constexpr int kWindowStride = kWindowBins + 1;
 
+// Stage the bins that positions [k0, k1) of the launch's order read (kSpan
+// bins from each step's first bin: 2 for the margin, 5 for the fraction)
+// into `window`; returns the number staged (0: none) and sets `first`, the
+// window's first bin.  In longitude order the body's azimuth moves
+// monotonically across a chunk, so the bins between those of its first and
+// last steps, plus the span and a margin of 2 on each side, cover it; a step
+// outside them reads its row directly.
+template <int kSpan>
+__device__ __forceinline__ int stage_window(const LightingBatch &B, const Frame32 &f,
+                                            const float *horizon, int k0, int k1, float *window,
+                                            int &first) {
+    if (!B.order || k1 <= k0) return 0;
+    float azimuth_deg, elevation;
+    const float *v = B.vectors + 3 * static_cast<size_t>(__ldg(B.order + k0));
+    body_direction(f, __ldg(v), __ldg(v + 1), __ldg(v + 2), azimuth_deg, elevation);
+    const int a = kSpan == 2 ? margin_position(azimuth_deg).left : sun_position(azimuth_deg).left;
+    v = B.vectors + 3 * static_cast<size_t>(__ldg(B.order + k1 - 1));
+    body_direction(f, __ldg(v), __ldg(v + 1), __ldg(v + 2), azimuth_deg, elevation);
+    const int b = kSpan == 2 ? margin_position(azimuth_deg).left : sun_position(azimuth_deg).left;
+    int arc = b - a;
+    if (arc < 0) arc += kAzimuths;
+    int start = arc <= kAzimuths / 2 ? a : b;
+    if (arc > kAzimuths / 2) arc = kAzimuths - arc;
+    start -= 2;
+    if (start < 0) start += kAzimuths;
+    if (arc + kSpan + 4 > kWindowBins) return 0;
+    first = start;
+    const int width = arc + kSpan + 4;
+    for (int i = 0; i < width; ++i) {
+        int bin = first + i;
+        if (bin >= kAzimuths) bin -= kAzimuths;
+        window[i] = __ldg(horizon + bin);
+    }
+    return width;
+}
+
+// Chunk length of an ordered launch: a chunk of c steps sweeps about
+// c * 1440 / T bins; keep that to 20 so its bins fit the staged window.
+static int ordered_chunk(int chunk, int time_count) {
+    return std::min(chunk, std::max(16, (kWindowBins - 12) * time_count / kAzimuths));
+}
+
 template <int kSignal>
 __global__ void __launch_bounds__(128) lighting_kernel(const __grid_constant__ LightingBatch B) {
     const int tile = blockIdx.z;
@@ -130,40 +172,11 @@ __global__ void __launch_bounds__(128) lighting_kernel(const __grid_constant__ L
 #pragma unroll
     for (int k = 0; k < 12; ++k) f.v[k] = src[k];
     const float *horizon = B.horizons + (static_cast<size_t>(tile) * plane + index) * kAzimuths;
-    // Stage the bins this chunk reads.  In longitude order the body's
-    // azimuth moves monotonically across a chunk, so the bins between those
-    // of its first and last steps (plus the signal's span and a margin of 2
-    // on each side) cover it; a step outside them reads its row directly.
     __shared__ float windows[128 * kWindowStride];
     float *window = windows + threadIdx.x * kWindowStride;
     constexpr int kSpan = kSignal == kSignalMargin ? 2 : 5;
-    int first = 0, width = 0;
-    if (B.order && k1 > k0) {
-        float azimuth_deg, elevation;
-        const float *v = B.vectors + 3 * static_cast<size_t>(__ldg(B.order + k0));
-        body_direction(f, __ldg(v), __ldg(v + 1), __ldg(v + 2), azimuth_deg, elevation);
-        const int a = kSignal == kSignalMargin ? margin_position(azimuth_deg).left
-                                               : sun_position(azimuth_deg).left;
-        v = B.vectors + 3 * static_cast<size_t>(__ldg(B.order + k1 - 1));
-        body_direction(f, __ldg(v), __ldg(v + 1), __ldg(v + 2), azimuth_deg, elevation);
-        const int b = kSignal == kSignalMargin ? margin_position(azimuth_deg).left
-                                               : sun_position(azimuth_deg).left;
-        int arc = b - a;
-        if (arc < 0) arc += kAzimuths;
-        int start = arc <= kAzimuths / 2 ? a : b;
-        if (arc > kAzimuths / 2) arc = kAzimuths - arc;
-        start -= 2;
-        if (start < 0) start += kAzimuths;
-        if (arc + kSpan + 4 <= kWindowBins) {
-            first = start;
-            width = arc + kSpan + 4;
-            for (int i = 0; i < width; ++i) {
-                int bin = first + i;
-                if (bin >= kAzimuths) bin -= kAzimuths;
-                window[i] = __ldg(horizon + bin);
-            }
-        }
-    }
+    int first = 0;
+    const int width = stage_window<kSpan>(B, f, horizon, k0, k1, window, first);
     for (int k = k0; k < k1; ++k) {
         const int t = B.order ? __ldg(B.order + k) : B.time_start + k;
         const float *v = B.vectors + 3 * static_cast<size_t>(t);
@@ -305,11 +318,7 @@ void lighting_launch(ls200_context *ctx, LightingBatch &B, int tiles, int signal
         psr_kernel<<<grid, 128, 0, ctx->stream>>>(B);
     } else {
         B.chunk = lighting_chunk(ctx, tiles, B.time_count);
-        // In longitude order a chunk of c steps sweeps about c * 1440 / T
-        // bins; keep that to 20 so the chunk's bins fit the staged window.
-        if (B.order)
-            B.chunk = std::min(B.chunk,
-                               std::max(16, (kWindowBins - 12) * B.time_count / kAzimuths));
+        if (B.order) B.chunk = ordered_chunk(B.chunk, B.time_count);
         dim3 grid(kPatch * kPatch / 128, (B.time_count + B.chunk - 1) / B.chunk, tiles);
         if (signal == kSignalFraction)
             lighting_kernel<kSignalFraction><<<grid, 128, 0, ctx->stream>>>(B);
@@ -362,48 +371,61 @@ void directions_launch(ls200_context *ctx, LightingBatch &B, int tiles, float2 *
 // the per-sample condition fraction >= sun_threshold, and with Earth vectors
 // earth margin >= earth_threshold), 32 time steps per word: bits
 // [tiles, 16384, words].  Same per-sample arithmetic as lighting_kernel.
+// Sun fraction at (azimuth, elevation) from a thread's staged window when it
+// holds the five bins, else from the pixel's row.
+__device__ __forceinline__ float staged_sun_fraction(const float *window, int first, int width,
+                                                     const float *horizon, float azimuth_deg,
+                                                     float elevation) {
+    const BinPosition p = sun_position(azimuth_deg);
+    int offset = p.left - first;
+    if (offset < 0) offset += kAzimuths;
+    return offset + 5 <= width
+               ? sun_fraction_bins(SharedBins{window, offset}, p.fraction, elevation)
+               : sun_fraction_bins(GlobalBins{horizon, p.left}, p.fraction, elevation);
+}
+
+// Condition bits word-major [tiles, words, 16384] (zeroed before the
+// launch): each thread visits a chunk of the Sun table's longitude order
+// with the Sun's bins staged, and sets the bits of the steps whose
+// condition holds (atomicOr: other chunks own the word's other steps).
 template <bool kEarth>
 __global__ void __launch_bounds__(128) condition_kernel(const __grid_constant__ LightingBatch B,
                                                         const float *__restrict__ earth,
                                                         float sun_threshold,
                                                         float earth_threshold, int words,
-                                                        int words_per_thread,
                                                         uint32_t *__restrict__ bits) {
     const int tile = blockIdx.z;
     const int index = blockIdx.x * blockDim.x + threadIdx.x;
     if (index >= kPatch * kPatch) return;
     const TileGeo &g = B.tiles[tile];
     const int sample = index % kPatch, line = index / kPatch;
+    if (sample >= g.valid_width || line >= g.valid_height) return;
     const size_t plane = static_cast<size_t>(kPatch) * kPatch;
-    uint32_t *row = bits + (static_cast<size_t>(tile) * plane + index) * words;
-    const int w0 = blockIdx.y * words_per_thread;
-    const int w1 = min(w0 + words_per_thread, words);
-    if (sample >= g.valid_width || line >= g.valid_height) {
-        for (int w = w0; w < w1; ++w) row[w] = 0u;
-        return;
-    }
+    uint32_t *tile_bits = bits + static_cast<size_t>(tile) * words * plane + index;
+    const int k0 = blockIdx.y * B.chunk;
+    const int k1 = min(k0 + B.chunk, B.time_count);
     Frame32 f;
     const float *src = B.frames + (static_cast<size_t>(tile) * plane + index) * 12;
 #pragma unroll
     for (int k = 0; k < 12; ++k) f.v[k] = src[k];
     const float *horizon = B.horizons + (static_cast<size_t>(tile) * plane + index) * kAzimuths;
-    for (int w = w0; w < w1; ++w) {
-        uint32_t word = 0u;
-        for (int j = 0; j < 32; ++j) {
-            const int t = w * 32 + j;
-            if (t >= B.time_count) break;
-            const float *v = B.vectors + 3 * static_cast<size_t>(t);
-            float azimuth_deg, elevation;
-            body_direction(f, __ldg(v), __ldg(v + 1), __ldg(v + 2), azimuth_deg, elevation);
-            bool on = sun_fraction(horizon, azimuth_deg, elevation) >= sun_threshold;
-            if (kEarth && on) {
-                const float *e = earth + 3 * static_cast<size_t>(t);
-                body_direction(f, __ldg(e), __ldg(e + 1), __ldg(e + 2), azimuth_deg, elevation);
-                on = horizon_margin(horizon, azimuth_deg, elevation) >= earth_threshold;
-            }
-            word |= static_cast<uint32_t>(on) << j;
+    __shared__ float windows[128 * kWindowStride];
+    float *window = windows + threadIdx.x * kWindowStride;
+    int first = 0;
+    const int width = stage_window<5>(B, f, horizon, k0, k1, window, first);
+    for (int k = k0; k < k1; ++k) {
+        const int t = B.order ? __ldg(B.order + k) : k;
+        const float *v = B.vectors + 3 * static_cast<size_t>(t);
+        float azimuth_deg, elevation;
+        body_direction(f, __ldg(v), __ldg(v + 1), __ldg(v + 2), azimuth_deg, elevation);
+        bool on = staged_sun_fraction(window, first, width, horizon, azimuth_deg, elevation) >=
+                  sun_threshold;
+        if (kEarth && on) {
+            const float *e = earth + 3 * static_cast<size_t>(t);
+            body_direction(f, __ldg(e), __ldg(e + 1), __ldg(e + 2), azimuth_deg, elevation);
+            on = horizon_margin(horizon, azimuth_deg, elevation) >= earth_threshold;
         }
-        row[w] = word;
+        if (on) atomicOr(tile_bits + static_cast<size_t>(t >> 5) * plane, 1u << (t & 31));
     }
 }
 
@@ -443,10 +465,12 @@ __global__ void __launch_bounds__(128) duration_kernel(const __grid_constant__ D
     const bool valid =
         index % kPatch < P.valid[tile].x && index / kPatch < P.valid[tile].y;
     if (valid) {
-        const uint32_t *row = P.bits + (static_cast<size_t>(tile) * plane + index) * P.words;
+        // Word-major bits: word w of this pixel at row[w * plane].
+        const uint32_t *row = P.bits + static_cast<size_t>(tile) * P.words * plane + index;
         int run_start = -1;
         for (int t = 0; t <= P.time_count; ++t) {
-            const bool on = t < P.time_count && ((row[t >> 5] >> (t & 31)) & 1u);
+            const bool on =
+                t < P.time_count && ((row[static_cast<size_t>(t >> 5) * plane] >> (t & 31)) & 1u);
             if (on) {
                 if (run_start < 0) run_start = t;
                 continue;
@@ -473,7 +497,8 @@ __global__ void __launch_bounds__(128) duration_kernel(const __grid_constant__ D
 void mission_duration_launch(ls200_context *ctx, LightingBatch &B, int tiles,
                              const float *earth, float sun_threshold, float earth_threshold,
                              uint32_t *bits, const double *hours, const double *prefix,
-                             const int2 *windows, int interval_count, bool days, float *out) {
+                             const int2 *windows, int interval_count, bool days, float *out,
+                             const int *order) {
     LS_REQUIRE(tiles >= 1 && tiles <= kMaxBatchTiles, "1 to 32 tiles per launch");
     LS_REQUIRE(interval_count >= 1 && interval_count <= kMaxDurationIntervals,
                "1 to 64 start intervals");
@@ -482,17 +507,19 @@ void mission_duration_launch(ls200_context *ctx, LightingBatch &B, int tiles,
     frames_kernel<<<grid_frames, 128, 0, ctx->stream>>>(B);
     LS_CUDA(cudaGetLastError());
     const int words = (B.time_count + 31) / 32;
-    const int chunk_steps = lighting_chunk(ctx, tiles, B.time_count);
-    const int words_per_thread = std::max(1, chunk_steps / 32);
-    dim3 grid(kPatch * kPatch / 128, (words + words_per_thread - 1) / words_per_thread, tiles);
+    LS_CUDA(cudaMemsetAsync(bits, 0,
+                            sizeof(uint32_t) * static_cast<size_t>(tiles) * words * kPatch * kPatch,
+                            ctx->stream));
+    B.order = order;
+    B.chunk = lighting_chunk(ctx, tiles, B.time_count);
+    if (B.order) B.chunk = ordered_chunk(B.chunk, B.time_count);
+    dim3 grid(kPatch * kPatch / 128, (B.time_count + B.chunk - 1) / B.chunk, tiles);
     if (earth)
         condition_kernel<true><<<grid, 128, 0, ctx->stream>>>(B, earth, sun_threshold,
-                                                             earth_threshold, words,
-                                                             words_per_thread, bits);
+                                                             earth_threshold, words, bits);
     else
         condition_kernel<false><<<grid, 128, 0, ctx->stream>>>(B, nullptr, sun_threshold,
-                                                              earth_threshold, words,
-                                                              words_per_thread, bits);
+                                                              earth_threshold, words, bits);
     LS_CUDA(cudaGetLastError());
     DurationParams P{};
     P.bits = bits;
@@ -518,46 +545,44 @@ void mission_duration_launch(ls200_context *ctx, LightingBatch &B, int tiles,
 // Same per-sample arithmetic as lighting_kernel.
 __global__ void __launch_bounds__(128) haven_condition_kernel(
     const __grid_constant__ LightingBatch B, const float *__restrict__ earth,
-    float sunlight_threshold, float earth_threshold, int words, int words_per_thread,
+    float sunlight_threshold, float earth_threshold, int words,
     uint32_t *__restrict__ low_bits, uint32_t *__restrict__ outage_bits) {
     const int tile = blockIdx.z;
     const int index = blockIdx.x * blockDim.x + threadIdx.x;
     if (index >= kPatch * kPatch) return;
     const TileGeo &g = B.tiles[tile];
     const int sample = index % kPatch, line = index / kPatch;
+    if (sample >= g.valid_width || line >= g.valid_height) return;
     const size_t plane = static_cast<size_t>(kPatch) * kPatch;
     const size_t base = static_cast<size_t>(tile) * words * plane + index;
-    const int w0 = blockIdx.y * words_per_thread;
-    const int w1 = min(w0 + words_per_thread, words);
-    if (sample >= g.valid_width || line >= g.valid_height) {
-        for (int w = w0; w < w1; ++w) {
-            low_bits[base + w * plane] = 0u;
-            outage_bits[base + w * plane] = 0u;
-        }
-        return;
-    }
+    // Bits were zeroed before the launch; the thread visits a chunk of the
+    // Sun table's longitude order (the Sun's bins staged) and sets the bits
+    // of its steps (atomicOr: other chunks own the word's other steps).
+    const int k0 = blockIdx.y * B.chunk;
+    const int k1 = min(k0 + B.chunk, B.time_count);
     Frame32 f;
     const float *src = B.frames + (static_cast<size_t>(tile) * plane + index) * 12;
 #pragma unroll
     for (int k = 0; k < 12; ++k) f.v[k] = src[k];
     const float *horizon = B.horizons + (static_cast<size_t>(tile) * plane + index) * kAzimuths;
-    for (int w = w0; w < w1; ++w) {
-        uint32_t low = 0u, outage = 0u;
-        for (int j = 0; j < 32; ++j) {
-            const int t = w * 32 + j;
-            if (t >= B.time_count) break;
-            const float *v = B.vectors + 3 * static_cast<size_t>(t);
-            float azimuth_deg, elevation;
-            body_direction(f, __ldg(v), __ldg(v + 1), __ldg(v + 2), azimuth_deg, elevation);
-            low |= static_cast<uint32_t>(sun_fraction(horizon, azimuth_deg, elevation) <
-                                         sunlight_threshold) << j;
-            const float *e = earth + 3 * static_cast<size_t>(t);
-            body_direction(f, __ldg(e), __ldg(e + 1), __ldg(e + 2), azimuth_deg, elevation);
-            outage |= static_cast<uint32_t>(horizon_margin(horizon, azimuth_deg, elevation) <
-                                            earth_threshold) << j;
-        }
-        low_bits[base + w * plane] = low;
-        outage_bits[base + w * plane] = outage;
+    __shared__ float windows[128 * kWindowStride];
+    float *window = windows + threadIdx.x * kWindowStride;
+    int first = 0;
+    const int width = stage_window<5>(B, f, horizon, k0, k1, window, first);
+    for (int k = k0; k < k1; ++k) {
+        const int t = B.order ? __ldg(B.order + k) : k;
+        const float *v = B.vectors + 3 * static_cast<size_t>(t);
+        float azimuth_deg, elevation;
+        body_direction(f, __ldg(v), __ldg(v + 1), __ldg(v + 2), azimuth_deg, elevation);
+        const size_t word = base + static_cast<size_t>(t >> 5) * plane;
+        const uint32_t bit = 1u << (t & 31);
+        if (staged_sun_fraction(window, first, width, horizon, azimuth_deg, elevation) <
+            sunlight_threshold)
+            atomicOr(low_bits + word, bit);
+        const float *e = earth + 3 * static_cast<size_t>(t);
+        body_direction(f, __ldg(e), __ldg(e + 1), __ldg(e + 2), azimuth_deg, elevation);
+        if (horizon_margin(horizon, azimuth_deg, elevation) < earth_threshold)
+            atomicOr(outage_bits + word, bit);
     }
 }
 
@@ -664,20 +689,21 @@ __global__ void __launch_bounds__(128) haven_kernel(const __grid_constant__ Have
 void safe_haven_launch(ls200_context *ctx, LightingBatch &B, int tiles, const float *earth,
                        float sunlight_threshold, float earth_threshold, uint32_t *bits,
                        const int *month, int bands, float hours, int *longest,
-                       uint8_t *flags, float *out) {
+                       uint8_t *flags, float *out, const int *order) {
     LS_REQUIRE(tiles >= 1 && tiles <= kMaxBatchTiles, "1 to 32 tiles per launch");
     ensure_lighting_constants(ctx);
     dim3 grid_frames(kPatch * kPatch / 128, tiles);
     frames_kernel<<<grid_frames, 128, 0, ctx->stream>>>(B);
     LS_CUDA(cudaGetLastError());
     const int words = (B.time_count + 31) / 32;
-    const int chunk_steps = lighting_chunk(ctx, tiles, B.time_count);
-    const int words_per_thread = std::max(1, chunk_steps / 32);
     const size_t stream_words = static_cast<size_t>(tiles) * words * kPatch * kPatch;
-    dim3 grid(kPatch * kPatch / 128, (words + words_per_thread - 1) / words_per_thread, tiles);
+    LS_CUDA(cudaMemsetAsync(bits, 0, sizeof(uint32_t) * 2 * stream_words, ctx->stream));
+    B.order = order;
+    B.chunk = lighting_chunk(ctx, tiles, B.time_count);
+    if (B.order) B.chunk = ordered_chunk(B.chunk, B.time_count);
+    dim3 grid(kPatch * kPatch / 128, (B.time_count + B.chunk - 1) / B.chunk, tiles);
     haven_condition_kernel<<<grid, 128, 0, ctx->stream>>>(B, earth, sunlight_threshold,
-                                                          earth_threshold, words,
-                                                          words_per_thread, bits,
+                                                          earth_threshold, words, bits,
                                                           bits + stream_words);
     LS_CUDA(cudaGetLastError());
     HavenParams P{};
@@ -711,19 +737,33 @@ __global__ void __launch_bounds__(128) visibility_kernel(const __grid_constant__
     const TileGeo &g = B.tiles[tile];
     if (index % kPatch >= g.valid_width || index / kPatch >= g.valid_height) return;
     const size_t plane = static_cast<size_t>(kPatch) * kPatch;
-    const int t0 = blockIdx.y * B.chunk;
-    const int t1 = min(t0 + B.chunk, B.time_count);
+    const int k0 = blockIdx.y * B.chunk;
+    const int k1 = min(k0 + B.chunk, B.time_count);
     Frame32 f;
     const float *src = B.frames + (static_cast<size_t>(tile) * plane + index) * 12;
 #pragma unroll
     for (int k = 0; k < 12; ++k) f.v[k] = src[k];
     const float *horizon = B.horizons + (static_cast<size_t>(tile) * plane + index) * kAzimuths;
+    // A count does not depend on the order of its steps: visit them in the
+    // table's longitude order with the chunk's bins staged (as lighting_kernel).
+    __shared__ float windows[128 * kWindowStride];
+    float *window = windows + threadIdx.x * kWindowStride;
+    int first = 0;
+    const int width = stage_window<2>(B, f, horizon, k0, k1, window, first);
     unsigned count = 0;
-    for (int t = t0; t < t1; ++t) {
+    for (int k = k0; k < k1; ++k) {
+        const int t = B.order ? __ldg(B.order + k) : k;
         const float *v = B.vectors + 3 * static_cast<size_t>(t);
         float azimuth_deg, elevation;
         body_direction(f, __ldg(v), __ldg(v + 1), __ldg(v + 2), azimuth_deg, elevation);
-        count += horizon_margin(horizon, azimuth_deg, elevation) >= threshold ? 1u : 0u;
+        const BinPosition p = margin_position(azimuth_deg);
+        int offset = p.left - first;
+        if (offset < 0) offset += kAzimuths;
+        const float margin =
+            offset + 2 <= width
+                ? horizon_margin_bins(SharedBins{window, offset}, p.fraction, elevation)
+                : horizon_margin_bins(GlobalBins{horizon, p.left}, p.fraction, elevation);
+        count += margin >= threshold ? 1u : 0u;
     }
     if (count) atomicAdd(counts + static_cast<size_t>(tile) * plane + index, count);
 }
@@ -739,15 +779,17 @@ __global__ void visibility_finalize(const unsigned *__restrict__ counts, int n, 
 }
 
 void visibility_launch(ls200_context *ctx, LightingBatch &B, int tiles, float threshold,
-                       unsigned *counts, int2 *valid, float *out) {
+                       unsigned *counts, int2 *valid, float *out, const int *order) {
     LS_REQUIRE(tiles >= 1 && tiles <= kMaxBatchTiles, "1 to 32 tiles per launch");
     ensure_lighting_constants(ctx);
+    B.order = order;
     const int n = tiles * kPatch * kPatch;
     LS_CUDA(cudaMemsetAsync(counts, 0, sizeof(unsigned) * n, ctx->stream));
     dim3 grid_frames(kPatch * kPatch / 128, tiles);
     frames_kernel<<<grid_frames, 128, 0, ctx->stream>>>(B);
     LS_CUDA(cudaGetLastError());
     B.chunk = lighting_chunk(ctx, tiles, B.time_count);
+    if (B.order) B.chunk = ordered_chunk(B.chunk, B.time_count);
     dim3 grid(kPatch * kPatch / 128, (B.time_count + B.chunk - 1) / B.chunk, tiles);
     visibility_kernel<<<grid, 128, 0, ctx->stream>>>(B, threshold, counts);
     LS_CUDA(cudaGetLastError());

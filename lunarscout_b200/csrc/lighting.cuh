@@ -62,33 +62,37 @@ void ensure_lighting_constants(ls200_context *ctx);
 void directions_launch(ls200_context *ctx, LightingBatch &batch, int tiles, float2 *out);
 // The mission-duration product fused with the lighting: per-pixel condition
 // bits (sun fraction >= sun_threshold [and, with `earth`, Earth margin >=
-// earth_threshold]) into `bits` ([tiles, 16384, ceil(T/32)] words), then the
+// earth_threshold]) into `bits` ([tiles, ceil(T/32), 16384] words), then the
 // longest right-censored run per start interval into out [tiles, I, 16384]
 // (hours, or days).  hours: device [T] sample durations; prefix: device
 // [T + 1] exact prefix sums or NULL; windows: device [I] (first, end) sample
-// indices of each start window.
+// indices of each start window; order: the Sun table's longitude order
+// (NULL: time order) in which the conditions are evaluated.
 void mission_duration_launch(ls200_context *ctx, LightingBatch &batch, int tiles,
                              const float *earth, float sun_threshold, float earth_threshold,
                              uint32_t *bits, const double *hours, const double *prefix,
-                             const int2 *windows, int interval_count, bool days, float *out);
+                             const int2 *windows, int interval_count, bool days, float *out,
+                             const int *order);
 
 // The safe-haven product fused with the lighting: low-Sun and Earth-outage
 // bits ([2, tiles, ceil(T/32), 16384] words in `bits`), then per pixel and
 // month band the longest low-Sun run that overlapped an outage in that band,
 // in hours, into out [tiles, bands, 16384] (NaN where the band is ill-posed).
 // month: device [T] band index per time step (-1 for none); longest and
-// flags: device scratch [tiles, bands, 16384].
+// flags: device scratch [tiles, bands, 16384]; order: the Sun table's
+// longitude order (NULL: time order) in which the bits are evaluated.
 void safe_haven_launch(ls200_context *ctx, LightingBatch &batch, int tiles, const float *earth,
                        float sunlight_threshold, float earth_threshold, uint32_t *bits,
                        const int *month, int bands, float hours, int *longest,
-                       uint8_t *flags, float *out);
+                       uint8_t *flags, float *out, const int *order);
 
 // Earth-visibility fraction: per pixel the share of the batch's time steps
 // whose Earth margin is >= threshold (degrees), into out [tiles, 16384] (NaN
 // outside the valid rectangle).  counts: device scratch [tiles, 16384];
-// valid: device [tiles] (valid width, valid height).
+// valid: device [tiles] (valid width, valid height); order: the table's
+// longitude order of the time steps (NULL: time order).
 void visibility_launch(ls200_context *ctx, LightingBatch &batch, int tiles, float threshold,
-                       unsigned *counts, int2 *valid, float *out);
+                       unsigned *counts, int2 *valid, float *out, const int *order);
 
 #ifdef LS200_LIGHTING_KERNELS
 // Slice half-heights and their normaliser (set by ensure_lighting_constants).

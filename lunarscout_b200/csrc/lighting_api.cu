@@ -310,7 +310,7 @@ ls200_status ls200_mission_duration_device(
         mission_duration_launch(ctx, B, tile_count, earth ? earth->data : nullptr,
                                 sun_threshold, earth_threshold, st.duration_bits.as<uint32_t>(),
                                 d_hours, integral ? d_prefix : nullptr, d_windows,
-                                interval_count, output_days != 0, out);
+                                interval_count, output_days != 0, out, sun->order);
         // The host tables above must outlive their copies.
         LS_CUDA(cudaStreamSynchronize(ctx->stream));
     });
@@ -375,7 +375,8 @@ ls200_status ls200_safe_haven_device(
         safe_haven_launch(ctx, B, tile_count, earth->data, sunlight_threshold,
                           earth_threshold_deg, st.haven_bits.as<uint32_t>(),
                           st.haven_months.as<int32_t>(), band_count, time_step_hours,
-                          st.haven_longest.as<int32_t>(), st.haven_flags.as<uint8_t>(), out);
+                          st.haven_longest.as<int32_t>(), st.haven_flags.as<uint8_t>(), out,
+                          sun->order);
         // The host month table must outlive its copy.
         LS_CUDA(cudaStreamSynchronize(ctx->stream));
     });
@@ -424,7 +425,7 @@ ls200_status ls200_earth_visibility_device(ls200_context *ctx, int tile_count,
         B.time_start = 0;
         B.time_count = earth->count;
         visibility_launch(ctx, B, tile_count, threshold_deg, st.visibility.as<unsigned>(),
-                          d_valid, out);
+                          d_valid, out, earth->order);
         // The host valid table must outlive its copy.
         LS_CUDA(cudaStreamSynchronize(ctx->stream));
     });

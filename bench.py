@@ -611,6 +611,7 @@ def multisite_pipeline(session, stream, grids, tiles, chosen, out, plain, batche
         batched_s = timed(batched_pipeline)
         plain_s = timed(plain_pipeline)
         lightmap_graph_s = timed(graph.launch)
+        graph_nodes = graph.nodes
     finally:
         graph.close()
         table.close()
@@ -618,7 +619,7 @@ def multisite_pipeline(session, stream, grids, tiles, chosen, out, plain, batche
     samples = sum(w[2] * w[3] for w in windows) * steps
     return {
         "tiles": count, "time_steps": steps, "chunk_steps": PIPELINE_CHUNK,
-        "graph_nodes_per_batch": len(blocks) * 2,
+        "graph_nodes_per_batch": graph_nodes,
         "batched_seconds": batched_s, "plain_seconds": plain_s,
         "speedup_batched_vs_plain": plain_s / batched_s,
         "batched_rays_per_s": rays / batched_s,

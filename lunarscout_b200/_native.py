@@ -199,6 +199,46 @@ def pinned_empty(shape, dtype=np.float32) -> np.ndarray:
     return np.frombuffer(buffer, dtype=dtype, count=count).reshape(shape)
 
 
+class PinnedPool:
+    """Page-locked host arrays that recycle their memory.
+
+    ``empty`` returns an ordinary writeable numpy array backed by pinned
+    memory.  When its last view dies the buffer returns to the pool (at most
+    ``keep`` idle buffers per size; others are freed), so a caller that drops
+    each result before the next call gets device-to-host copies at full DMA
+    speed into memory that is already mapped, instead of a fresh pageable
+    array faulted in page by page."""
+
+    def __init__(self, keep: int = 2) -> None:
+        self._idle: dict[int, list[int]] = {}
+        self._keep = keep
+        self._lock = threading.Lock()
+
+    def empty(self, shape, dtype=np.float32) -> np.ndarray:
+        dtype = np.dtype(dtype)
+        shape = tuple(int(s) for s in shape) if not isinstance(shape, int) else (shape,)
+        count = int(np.prod(shape, dtype=np.int64))
+        nbytes = max(count * dtype.itemsize, 1)
+        with self._lock:
+            stack = self._idle.get(nbytes)
+            address = stack.pop() if stack else None
+        if address is None:
+            pointer = ctypes.c_void_p()
+            call("ls200_host_alloc", nbytes, ctypes.byref(pointer))
+            address = pointer.value
+        buffer = (ctypes.c_byte * nbytes).from_address(address)
+        weakref.finalize(buffer, self._release, address, nbytes)
+        return np.frombuffer(buffer, dtype=dtype, count=count).reshape(shape)
+
+    def _release(self, address: int, nbytes: int) -> None:
+        with self._lock:
+            stack = self._idle.setdefault(nbytes, [])
+            if len(stack) < self._keep:
+                stack.append(address)
+                return
+        _free_host(address)
+
+
 def _free_host(address: int) -> None:
     try:
         library().ls200_host_free(ctypes.c_void_p(address))

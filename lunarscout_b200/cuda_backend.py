@@ -29,6 +29,10 @@ __all__ = ["CudaBackendError", "CudaExecutionError", "CudaDeviceInfo", "CudaSess
 #: Traversals of the batched march: the reference's, and the skip ladder.
 TRAVERSALS = {"exact": 0, "ladder": 1}
 
+# Slope arrays returned by the march calls live in recycled pinned memory
+# (fresh, ordinary numpy arrays to the caller).
+_OUTPUTS = _native.PinnedPool(keep=2)
+
 
 @dataclass(frozen=True, slots=True)
 class CudaDeviceInfo:
@@ -276,7 +280,7 @@ class CudaSession:
         primary = self.upload_pyramid(primary_pyramid)
         active = primary if active_pyramid is primary_pyramid else self.upload_pyramid(
             active_pyramid)
-        out = np.empty(output_shape, dtype=np.float32)
+        out = _OUTPUTS.empty(output_shape, np.float32)
         try:
             call("ls200_march_pass", self._ctx, segments, segments.shape[0], segments.shape[1],
                  segments.shape[2], primary.handle, active.handle, int(tile_column),
@@ -301,7 +305,7 @@ class CudaSession:
             raise ValueError("pyramid count must match the segment DEM axis")
         dems = self._prepare_production_pyramids(pyramids)
         handles = (ctypes.c_void_p * len(dems))(*[d.handle.value for d in dems])
-        out = np.empty((tile_width * tile_height, segments.shape[0]), dtype=np.float32)
+        out = _OUTPUTS.empty((tile_width * tile_height, segments.shape[0]), np.float32)
         seconds = np.zeros(len(dems), dtype=np.float64)
         started = time.perf_counter()
         call("ls200_march_all_passes", self._ctx, segments, segments.shape[0],

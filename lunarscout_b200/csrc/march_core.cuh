@@ -41,7 +41,7 @@ struct LevelTable {
     float side[kMaxLevels];      // float(4^l) * resolution: the level choice
     float fallback[kMaxLevels];  // ((side * 0.5) * 0.001)
     float out_step[kMaxLevels];  // max(0.001, side * 0.001)
-    int4 cells[kMaxLevels];      // (cell offset, width, height, -)
+    int4 cells[kMaxLevels];      // (cell offset, width, height, fallback bits)
 };
 
 // Everything the march of one DEM pass needs about the DEM.
@@ -91,7 +91,14 @@ __device__ __forceinline__ void fill_level(LevelTable &table, int l, float resol
     table.side[l] = block_m;
     table.fallback[l] = __fmul_rn(__fmul_rn(block_m, 0.5f), 0.001f);
     table.out_step[l] = 0.001f > step_km ? 0.001f : step_km;
-    table.cells[l] = cells;
+    // w carries the fallback's bits: a visit reads its cells and its
+    // fallback with one 16-byte load.
+    table.cells[l] = make_int4(cells.x, cells.y, cells.z, __float_as_int(table.fallback[l]));
+}
+
+// 2^shift as a float (exact; shift <= 38), from the exponent bits.
+__device__ __forceinline__ float power_of_two(int shift) {
+    return __int_as_float((127 + shift) << 23);
 }
 
 __device__ __forceinline__ float quartic(float x0, float a1, float a2, float a3, float a4,
@@ -249,7 +256,7 @@ __device__ __forceinline__ float cell_bound(const float *__restrict__ bounds, in
 // (bitwise the same value, including the -0.0 of a ray starting on the edge).
 __device__ __forceinline__ float cell_exit_advance(int shift, int cx, int cy, float px, float py,
                                                    float inv_x, float inv_y, float fallback) {
-    const float scale_f = static_cast<float>(1 << shift);
+    const float scale_f = power_of_two(shift);
     const float min_x = static_cast<float>(cx << shift);
     const float min_y = static_cast<float>(cy << shift);
     const float edge_x = inv_x > 0.0f ? __fadd_rn(min_x, scale_f) : min_x;
@@ -290,8 +297,9 @@ __device__ __forceinline__ bool ladder_culled(const Table &table, const float *_
                                               float current, float &step) {
     const int shift = 2 * m;
     const int cx = ipx >> shift, cy = ipy >> shift;
-    const float maximum_height = cell_bound(bounds, table.cells(m), cx, cy);
-    step = cell_exit_advance(shift, cx, cy, px, py, inv_x, inv_y, table.fallback(m));
+    const int4 L = table.cells(m);
+    const float maximum_height = cell_bound(bounds, L, cx, cy);
+    step = cell_exit_advance(shift, cx, cy, px, py, inv_x, inv_y, __int_as_float(L.w));
     if (maximum_height < -20000.0f) return true;
     const float dh = __fsub_rn(maximum_height, observer_z);
     const float far_distance = __fadd_rn(__fadd_rn(true_m, __fmul_rn(step, 1010.0f)), 1.0f);
@@ -541,10 +549,10 @@ __device__ __forceinline__ bool march_step_tracked(const Table &table, const Dem
             }
             const float maximum_height = cell_bound(dem.bounds, L, cx, cy);
             const float skip =
-                cell_exit_advance(shift, cx, cy, px, py, inv_x, inv_y, table.fallback(level));
+                cell_exit_advance(shift, cx, cy, px, py, inv_x, inv_y, __int_as_float(L.w));
             bool culled = maximum_height < -20000.0f;
             if (!culled) {
-                const float scale_f = static_cast<float>(1 << shift);
+                const float scale_f = power_of_two(shift);
                 float true_near = __fmaf_rn(-scale_f, resolution, true_m);
                 true_near = true_near > 1.0f ? true_near : 1.0f;
                 culled = bound_culled(near, true_near, maximum_height, radius, observer_z,

@@ -104,3 +104,41 @@ def test_capture_needs_a_created_stream(cuda_session):
             DeviceGraph.capture(cuda_session.context, lambda: None)
     finally:
         cuda_session.set_stream(None)
+
+
+def test_ordered_sub_ranges_equal_the_whole_launch_and_time_order(cuda_session,
+                                                                     lighting_inputs):
+    """Chunks of the time axis (each visiting its steps in longitude order
+    through the compacted order window) equal one whole-axis launch, which
+    equals time-order evaluation (the per-patch session, 32 steps a call)."""
+    import torch
+
+    from lunarscout_b200 import _native, synthetic
+    from lunarscout_b200.lightmap_cuda import LightmapCudaSession
+
+    inputs = lighting_inputs
+    outs = _outputs(inputs)
+    _chunks(cuda_session, inputs, outs)
+    total = sum(count for _, count in inputs["blocks"])
+    whole = torch.zeros((TILES, total, 128 * 128), dtype=torch.uint8, device="cuda")
+    _native.check(_native.library().ls200_lighting_device(
+        cuda_session.context, TILES, ctypes.c_void_p(inputs["patches"].data_ptr()),
+        inputs["geo"].ctypes.data, inputs["proj"].ctypes.data, inputs["windows"].ctypes.data,
+        ctypes.c_void_p(inputs["horizons"].data_ptr()), inputs["table"].handle, 0, total, 1,
+        ctypes.c_void_p(inputs["frames"].data_ptr()), ctypes.c_void_p(whole.data_ptr())))
+    cuda_session.synchronize()
+    torch.cuda.synchronize()
+    np.testing.assert_array_equal(torch.cat(outs, dim=1).cpu().numpy(), whole.cpu().numpy())
+    dem = synthetic.config1_dem()
+    hours = synthetic.hours_between("2030-01-01T00", "2030-05-01T00", 1.0)[:total]
+    session = LightmapCudaSession(time_batch_size=32)
+    try:
+        tile_x, tile_y, vw, vh = (int(v) for v in inputs["windows"][1])
+        horizons = inputs["horizons"][1].view(128, 128, 1440).cpu().numpy()
+        expected = np.stack(list(session.iter_patch_tiles(
+            dem, horizons, synthetic.sun_vectors(hours), tile_y=tile_y, tile_x=tile_x,
+            valid_height=vh, valid_width=vw)))
+    finally:
+        session.close()
+    got = whole[1].cpu().numpy().reshape(total, 128, 128)[:, :vh, :vw]
+    np.testing.assert_array_equal(got, expected)

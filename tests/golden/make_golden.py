@@ -1,7 +1,7 @@
 """Generate the committed golden fixtures under tests/golden/.
 
-Run in a container that has the reference checkout (read-only) at
-REFERENCE_ROOT; the GPU box never runs this.  It imports the reference's own
+Run on a machine that has the reference checkout (read-only) at
+REFERENCE_ROOT; the tests only read its outputs.  It imports the reference's own
 Python modules through a stub package (its top-level ``__init__`` needs
 pyproj/rasterio, absent here) and extracts:
 

@@ -1,6 +1,6 @@
 """Lightmap (fraction, bytes, margin) and PSR on the B200 vs the oracle.
 
-Tolerances are the north-star bars: sun fraction within 1e-4 absolute of the
+Tolerances are the path's accuracy targets: sun fraction within 1e-4 absolute of the
 reference CPU backend; PSR bit-exact except a counted band of pixels whose
 peak (sun centre - horizon) lies within 1e-4 deg of the -0.2725 deg limb
 threshold.  Differences come only from CUDA's atan2f vs glibc's.

@@ -467,10 +467,13 @@ def multisite_benchmark(session, stream, args, world, rank):
                                             observer_elevation_m=OBSERVER_M,
                                             device_out=out[i].data_ptr(), degrees=True)
 
+    splits = {}  # traversal -> [(segment + setup seconds, march seconds)] per call
+
     def batched(traversal):
         def run(tiles):
-            session.march_sites(tiles, device_out=out.data_ptr(), azimuth_count=AZIMUTHS,
-                                traversal=traversal, degrees=True)
+            splits.setdefault(traversal, []).append(session.march_sites(
+                tiles, device_out=out.data_ptr(), azimuth_count=AZIMUTHS, traversal=traversal,
+                degrees=True))
         return run
 
     def timed(run):
@@ -501,6 +504,10 @@ def multisite_benchmark(session, stream, args, world, rank):
         "speedup_batched_vs_plain": ladder_value / plain_value,
         "speedup_exact_vs_plain": exact_value / plain_value,
         "seconds": {"plain": plain_s, "exact": exact_s, "ladder": ladder_s},
+        "batched_split_seconds": {
+            traversal: {"segments_and_setup": sum(s for s, _ in calls[-(SITE_BATCHES - 1):]),
+                        "march": sum(m for _, m in calls[-(SITE_BATCHES - 1):])}
+            for traversal, calls in splits.items()},
         "launch_config": {"lanes_per_azimuth": tuned.best.lanes_per_azimuth,
                           "min_blocks": tuned.best.min_blocks,
                           "tuned_on": f"{TUNE_TILES} tiles of the warm-up batch, ladder",

@@ -367,10 +367,6 @@ void directions_launch(ls200_context *ctx, LightingBatch &B, int tiles, float2 *
     LS_CUDA(cudaGetLastError());
 }
 
-// Condition bits of the mission-duration product (nh/mission_duration_pipeline.py:
-// the per-sample condition fraction >= sun_threshold, and with Earth vectors
-// earth margin >= earth_threshold), 32 time steps per word: bits
-// [tiles, 16384, words].  Same per-sample arithmetic as lighting_kernel.
 // Sun fraction at (azimuth, elevation) from a thread's staged window when it
 // holds the five bins, else from the pixel's row.
 __device__ __forceinline__ float staged_sun_fraction(const float *window, int first, int width,
@@ -384,16 +380,29 @@ __device__ __forceinline__ float staged_sun_fraction(const float *window, int fi
                : sun_fraction_bins(GlobalBins{horizon, p.left}, p.fraction, elevation);
 }
 
-// Condition bits word-major [tiles, words, 16384] (zeroed before the
-// launch): each thread visits a chunk of the Sun table's longitude order
-// with the Sun's bins staged, and sets the bits of the steps whose
-// condition holds (atomicOr: other chunks own the word's other steps).
-template <bool kEarth>
-__global__ void __launch_bounds__(128) condition_kernel(const __grid_constant__ LightingBatch B,
-                                                        const float *__restrict__ earth,
-                                                        float sun_threshold,
-                                                        float earth_threshold, int words,
-                                                        uint32_t *__restrict__ bits) {
+// The same for the margin (two bins).
+__device__ __forceinline__ float staged_margin(const float *window, int first, int width,
+                                               const float *horizon, float azimuth_deg,
+                                               float elevation) {
+    const BinPosition p = margin_position(azimuth_deg);
+    int offset = p.left - first;
+    if (offset < 0) offset += kAzimuths;
+    return offset + 2 <= width
+               ? horizon_margin_bins(SharedBins{window, offset}, p.fraction, elevation)
+               : horizon_margin_bins(GlobalBins{horizon, p.left}, p.fraction, elevation);
+}
+
+// Threshold bits of one signal of one body, word-major [tiles, words, 16384]
+// (zeroed before the launch): bit t is set where signal >= threshold
+// (kAtLeast) or signal < threshold.  kSpan 5 is the sun fraction, 2 the
+// margin.  Each thread visits a chunk of the body's table in its longitude
+// order with the chunk's bins staged, and sets the bits of its steps with
+// atomicOr (other chunks own the word's other steps).  Each signal runs in
+// its own body's order, so the Earth's reads are staged as well as the Sun's.
+template <int kSpan, bool kAtLeast>
+__global__ void __launch_bounds__(128) signal_bits_kernel(const __grid_constant__ LightingBatch B,
+                                                          float threshold, int words,
+                                                          uint32_t *__restrict__ bits) {
     const int tile = blockIdx.z;
     const int index = blockIdx.x * blockDim.x + threadIdx.x;
     if (index >= kPatch * kPatch) return;
@@ -412,21 +421,37 @@ __global__ void __launch_bounds__(128) condition_kernel(const __grid_constant__ 
     __shared__ float windows[128 * kWindowStride];
     float *window = windows + threadIdx.x * kWindowStride;
     int first = 0;
-    const int width = stage_window<5>(B, f, horizon, k0, k1, window, first);
+    const int width = stage_window<kSpan>(B, f, horizon, k0, k1, window, first);
     for (int k = k0; k < k1; ++k) {
         const int t = B.order ? __ldg(B.order + k) : k;
         const float *v = B.vectors + 3 * static_cast<size_t>(t);
         float azimuth_deg, elevation;
         body_direction(f, __ldg(v), __ldg(v + 1), __ldg(v + 2), azimuth_deg, elevation);
-        bool on = staged_sun_fraction(window, first, width, horizon, azimuth_deg, elevation) >=
-                  sun_threshold;
-        if (kEarth && on) {
-            const float *e = earth + 3 * static_cast<size_t>(t);
-            body_direction(f, __ldg(e), __ldg(e + 1), __ldg(e + 2), azimuth_deg, elevation);
-            on = horizon_margin(horizon, azimuth_deg, elevation) >= earth_threshold;
-        }
+        const float value =
+            kSpan == 5 ? staged_sun_fraction(window, first, width, horizon, azimuth_deg, elevation)
+                       : staged_margin(window, first, width, horizon, azimuth_deg, elevation);
+        const bool on = kAtLeast ? value >= threshold : value < threshold;
         if (on) atomicOr(tile_bits + static_cast<size_t>(t >> 5) * plane, 1u << (t & 31));
     }
+}
+
+// Zero `bits` ([tiles, words, 16384] words) and set the threshold bits of
+// one signal: `table` (vectors and their longitude order, or NULL for time
+// order) replaces the batch's vectors; the frames are already in place.
+template <int kSpan, bool kAtLeast>
+static void signal_bits_launch(ls200_context *ctx, LightingBatch B, int tiles,
+                               const float *vectors, const int *order, float threshold,
+                               int words, uint32_t *bits) {
+    LS_CUDA(cudaMemsetAsync(bits, 0,
+                            sizeof(uint32_t) * static_cast<size_t>(tiles) * words * kPatch * kPatch,
+                            ctx->stream));
+    B.vectors = vectors;
+    B.order = order;
+    B.chunk = lighting_chunk(ctx, tiles, B.time_count);
+    if (B.order) B.chunk = ordered_chunk(B.chunk, B.time_count);
+    dim3 grid(kPatch * kPatch / 128, (B.time_count + B.chunk - 1) / B.chunk, tiles);
+    signal_bits_kernel<kSpan, kAtLeast><<<grid, 128, 0, ctx->stream>>>(B, threshold, words, bits);
+    LS_CUDA(cudaGetLastError());
 }
 
 // Longest right-censored candidate run per start interval
@@ -439,7 +464,8 @@ __global__ void __launch_bounds__(128) condition_kernel(const __grid_constant__ 
 constexpr int kMaxDurationIntervals = 64;
 
 struct DurationParams {
-    const uint32_t *bits;
+    const uint32_t *bits;        // [tiles, words, 16384] sun fraction >= threshold
+    const uint32_t *earth_bits;  // the same for Earth margin >= threshold, or NULL
     const double *hours;   // [T] sample durations
     const double *prefix;  // [T + 1] exact prefix sums, or NULL
     const int2 *windows;   // [I] (first, end) sample indices of each start window
@@ -465,12 +491,16 @@ __global__ void __launch_bounds__(128) duration_kernel(const __grid_constant__ D
     const bool valid =
         index % kPatch < P.valid[tile].x && index / kPatch < P.valid[tile].y;
     if (valid) {
-        // Word-major bits: word w of this pixel at row[w * plane].
-        const uint32_t *row = P.bits + static_cast<size_t>(tile) * P.words * plane + index;
+        // Word-major bits: word w of this pixel at row[w * plane].  The
+        // condition is the Sun bit, and with Earth vectors also the Earth bit.
+        const size_t offset = static_cast<size_t>(tile) * P.words * plane + index;
+        const uint32_t *row = P.bits + offset;
+        const uint32_t *earth_row = P.earth_bits ? P.earth_bits + offset : nullptr;
         int run_start = -1;
         for (int t = 0; t <= P.time_count; ++t) {
-            const bool on =
-                t < P.time_count && ((row[static_cast<size_t>(t >> 5) * plane] >> (t & 31)) & 1u);
+            const size_t word = static_cast<size_t>(t >> 5) * plane;
+            const bool on = t < P.time_count && ((row[word] >> (t & 31)) & 1u) &&
+                            (!earth_row || ((earth_row[word] >> (t & 31)) & 1u));
             if (on) {
                 if (run_start < 0) run_start = t;
                 continue;
@@ -498,7 +528,7 @@ void mission_duration_launch(ls200_context *ctx, LightingBatch &B, int tiles,
                              const float *earth, float sun_threshold, float earth_threshold,
                              uint32_t *bits, const double *hours, const double *prefix,
                              const int2 *windows, int interval_count, bool days, float *out,
-                             const int *order) {
+                             const int *order, const int *earth_order) {
     LS_REQUIRE(tiles >= 1 && tiles <= kMaxBatchTiles, "1 to 32 tiles per launch");
     LS_REQUIRE(interval_count >= 1 && interval_count <= kMaxDurationIntervals,
                "1 to 64 start intervals");
@@ -507,22 +537,14 @@ void mission_duration_launch(ls200_context *ctx, LightingBatch &B, int tiles,
     frames_kernel<<<grid_frames, 128, 0, ctx->stream>>>(B);
     LS_CUDA(cudaGetLastError());
     const int words = (B.time_count + 31) / 32;
-    LS_CUDA(cudaMemsetAsync(bits, 0,
-                            sizeof(uint32_t) * static_cast<size_t>(tiles) * words * kPatch * kPatch,
-                            ctx->stream));
-    B.order = order;
-    B.chunk = lighting_chunk(ctx, tiles, B.time_count);
-    if (B.order) B.chunk = ordered_chunk(B.chunk, B.time_count);
-    dim3 grid(kPatch * kPatch / 128, (B.time_count + B.chunk - 1) / B.chunk, tiles);
+    const size_t stream_words = static_cast<size_t>(tiles) * words * kPatch * kPatch;
+    signal_bits_launch<5, true>(ctx, B, tiles, B.vectors, order, sun_threshold, words, bits);
     if (earth)
-        condition_kernel<true><<<grid, 128, 0, ctx->stream>>>(B, earth, sun_threshold,
-                                                             earth_threshold, words, bits);
-    else
-        condition_kernel<false><<<grid, 128, 0, ctx->stream>>>(B, nullptr, sun_threshold,
-                                                              earth_threshold, words, bits);
-    LS_CUDA(cudaGetLastError());
+        signal_bits_launch<2, true>(ctx, B, tiles, earth, earth_order, earth_threshold, words,
+                                    bits + stream_words);
     DurationParams P{};
     P.bits = bits;
+    P.earth_bits = earth ? bits + stream_words : nullptr;
     P.hours = hours;
     P.prefix = prefix;
     P.windows = windows;
@@ -536,54 +558,6 @@ void mission_duration_launch(ls200_context *ctx, LightingBatch &B, int tiles,
         P.valid[t] = make_int2(B.tiles[t].valid_width, B.tiles[t].valid_height);
     duration_kernel<<<dim3(kPatch * kPatch / 128, tiles), 128, 0, ctx->stream>>>(P);
     LS_CUDA(cudaGetLastError());
-}
-
-// Condition bits of the safe-haven product (safe_haven.py:156-160): per pixel
-// and time step, low Sun (sun fraction < sunlight_threshold) and Earth outage
-// (Earth margin < earth_threshold, degrees).  Word-major [tiles, words, 16384]:
-// a warp's 32 pixels write, and the reducer reads, 128 contiguous bytes.
-// Same per-sample arithmetic as lighting_kernel.
-__global__ void __launch_bounds__(128) haven_condition_kernel(
-    const __grid_constant__ LightingBatch B, const float *__restrict__ earth,
-    float sunlight_threshold, float earth_threshold, int words,
-    uint32_t *__restrict__ low_bits, uint32_t *__restrict__ outage_bits) {
-    const int tile = blockIdx.z;
-    const int index = blockIdx.x * blockDim.x + threadIdx.x;
-    if (index >= kPatch * kPatch) return;
-    const TileGeo &g = B.tiles[tile];
-    const int sample = index % kPatch, line = index / kPatch;
-    if (sample >= g.valid_width || line >= g.valid_height) return;
-    const size_t plane = static_cast<size_t>(kPatch) * kPatch;
-    const size_t base = static_cast<size_t>(tile) * words * plane + index;
-    // Bits were zeroed before the launch; the thread visits a chunk of the
-    // Sun table's longitude order (the Sun's bins staged) and sets the bits
-    // of its steps (atomicOr: other chunks own the word's other steps).
-    const int k0 = blockIdx.y * B.chunk;
-    const int k1 = min(k0 + B.chunk, B.time_count);
-    Frame32 f;
-    const float *src = B.frames + (static_cast<size_t>(tile) * plane + index) * 12;
-#pragma unroll
-    for (int k = 0; k < 12; ++k) f.v[k] = src[k];
-    const float *horizon = B.horizons + (static_cast<size_t>(tile) * plane + index) * kAzimuths;
-    __shared__ float windows[128 * kWindowStride];
-    float *window = windows + threadIdx.x * kWindowStride;
-    int first = 0;
-    const int width = stage_window<5>(B, f, horizon, k0, k1, window, first);
-    for (int k = k0; k < k1; ++k) {
-        const int t = B.order ? __ldg(B.order + k) : k;
-        const float *v = B.vectors + 3 * static_cast<size_t>(t);
-        float azimuth_deg, elevation;
-        body_direction(f, __ldg(v), __ldg(v + 1), __ldg(v + 2), azimuth_deg, elevation);
-        const size_t word = base + static_cast<size_t>(t >> 5) * plane;
-        const uint32_t bit = 1u << (t & 31);
-        if (staged_sun_fraction(window, first, width, horizon, azimuth_deg, elevation) <
-            sunlight_threshold)
-            atomicOr(low_bits + word, bit);
-        const float *e = earth + 3 * static_cast<size_t>(t);
-        body_direction(f, __ldg(e), __ldg(e + 1), __ldg(e + 2), azimuth_deg, elevation);
-        if (horizon_margin(horizon, azimuth_deg, elevation) < earth_threshold)
-            atomicOr(outage_bits + word, bit);
-    }
 }
 
 // Per-pixel safe-haven reducer (safe_haven.py:75-243), one thread per pixel
@@ -689,7 +663,8 @@ __global__ void __launch_bounds__(128) haven_kernel(const __grid_constant__ Have
 void safe_haven_launch(ls200_context *ctx, LightingBatch &B, int tiles, const float *earth,
                        float sunlight_threshold, float earth_threshold, uint32_t *bits,
                        const int *month, int bands, float hours, int *longest,
-                       uint8_t *flags, float *out, const int *order) {
+                       uint8_t *flags, float *out, const int *order,
+                       const int *earth_order) {
     LS_REQUIRE(tiles >= 1 && tiles <= kMaxBatchTiles, "1 to 32 tiles per launch");
     ensure_lighting_constants(ctx);
     dim3 grid_frames(kPatch * kPatch / 128, tiles);
@@ -697,15 +672,12 @@ void safe_haven_launch(ls200_context *ctx, LightingBatch &B, int tiles, const fl
     LS_CUDA(cudaGetLastError());
     const int words = (B.time_count + 31) / 32;
     const size_t stream_words = static_cast<size_t>(tiles) * words * kPatch * kPatch;
-    LS_CUDA(cudaMemsetAsync(bits, 0, sizeof(uint32_t) * 2 * stream_words, ctx->stream));
-    B.order = order;
-    B.chunk = lighting_chunk(ctx, tiles, B.time_count);
-    if (B.order) B.chunk = ordered_chunk(B.chunk, B.time_count);
-    dim3 grid(kPatch * kPatch / 128, (B.time_count + B.chunk - 1) / B.chunk, tiles);
-    haven_condition_kernel<<<grid, 128, 0, ctx->stream>>>(B, earth, sunlight_threshold,
-                                                          earth_threshold, words, bits,
-                                                          bits + stream_words);
-    LS_CUDA(cudaGetLastError());
+    // Low Sun (fraction < threshold) in the Sun's order, Earth outage
+    // (margin < threshold) in the Earth's (safe_haven.py:156-160).
+    signal_bits_launch<5, false>(ctx, B, tiles, B.vectors, order, sunlight_threshold, words,
+                                 bits);
+    signal_bits_launch<2, false>(ctx, B, tiles, earth, earth_order, earth_threshold, words,
+                                 bits + stream_words);
     HavenParams P{};
     P.low = bits;
     P.outage = bits + stream_words;

@@ -62,29 +62,31 @@ void ensure_lighting_constants(ls200_context *ctx);
 void directions_launch(ls200_context *ctx, LightingBatch &batch, int tiles, float2 *out);
 // The mission-duration product fused with the lighting: per-pixel condition
 // bits (sun fraction >= sun_threshold [and, with `earth`, Earth margin >=
-// earth_threshold]) into `bits` ([tiles, ceil(T/32), 16384] words), then the
-// longest right-censored run per start interval into out [tiles, I, 16384]
-// (hours, or days).  hours: device [T] sample durations; prefix: device
-// [T + 1] exact prefix sums or NULL; windows: device [I] (first, end) sample
-// indices of each start window; order: the Sun table's longitude order
-// (NULL: time order) in which the conditions are evaluated.
+// earth_threshold]) into `bits` ([tiles, ceil(T/32), 16384] words per
+// signal: room for two with `earth`), then the longest right-censored run
+// per start interval into out [tiles, I, 16384] (hours, or days).  hours:
+// device [T] sample durations; prefix: device [T + 1] exact prefix sums or
+// NULL; windows: device [I] (first, end) sample indices of each start
+// window; order / earth_order: the Sun's / Earth's table in longitude order
+// (NULL: time order), the order in which each signal is evaluated.
 void mission_duration_launch(ls200_context *ctx, LightingBatch &batch, int tiles,
                              const float *earth, float sun_threshold, float earth_threshold,
                              uint32_t *bits, const double *hours, const double *prefix,
                              const int2 *windows, int interval_count, bool days, float *out,
-                             const int *order);
+                             const int *order, const int *earth_order);
 
 // The safe-haven product fused with the lighting: low-Sun and Earth-outage
 // bits ([2, tiles, ceil(T/32), 16384] words in `bits`), then per pixel and
 // month band the longest low-Sun run that overlapped an outage in that band,
 // in hours, into out [tiles, bands, 16384] (NaN where the band is ill-posed).
 // month: device [T] band index per time step (-1 for none); longest and
-// flags: device scratch [tiles, bands, 16384]; order: the Sun table's
-// longitude order (NULL: time order) in which the bits are evaluated.
+// flags: device scratch [tiles, bands, 16384]; order / earth_order: the
+// Sun's / Earth's table in longitude order (NULL: time order), the order in
+// which each body's bits are evaluated.
 void safe_haven_launch(ls200_context *ctx, LightingBatch &batch, int tiles, const float *earth,
                        float sunlight_threshold, float earth_threshold, uint32_t *bits,
                        const int *month, int bands, float hours, int *longest,
-                       uint8_t *flags, float *out, const int *order);
+                       uint8_t *flags, float *out, const int *order, const int *earth_order);
 
 // Earth-visibility fraction: per pixel the share of the batch's time steps
 // whose Earth margin is >= threshold (degrees), into out [tiles, 16384] (NaN

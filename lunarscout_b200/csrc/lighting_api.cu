@@ -285,7 +285,8 @@ ls200_status ls200_mission_duration_device(
         const size_t plane = static_cast<size_t>(kPatch) * kPatch;
         const size_t words = (static_cast<size_t>(count) + 31) / 32;
         const size_t frames_bytes = sizeof(float) * 12 * tile_count * plane;
-        const size_t bits_bytes = sizeof(uint32_t) * tile_count * plane * words;
+        // One bit stream for the Sun's condition, a second for the Earth's.
+        const size_t bits_bytes = sizeof(uint32_t) * tile_count * plane * words * (earth ? 2 : 1);
         const size_t table_bytes = sizeof(double) * (2 * size_t(count) + 1) +
                                    sizeof(int2) * interval_count;
         st.duration_frames.reserve(frames_bytes);
@@ -310,7 +311,8 @@ ls200_status ls200_mission_duration_device(
         mission_duration_launch(ctx, B, tile_count, earth ? earth->data : nullptr,
                                 sun_threshold, earth_threshold, st.duration_bits.as<uint32_t>(),
                                 d_hours, integral ? d_prefix : nullptr, d_windows,
-                                interval_count, output_days != 0, out, sun->order);
+                                interval_count, output_days != 0, out, sun->order,
+                                earth ? earth->order : nullptr);
         // The host tables above must outlive their copies.
         LS_CUDA(cudaStreamSynchronize(ctx->stream));
     });
@@ -376,7 +378,7 @@ ls200_status ls200_safe_haven_device(
                           earth_threshold_deg, st.haven_bits.as<uint32_t>(),
                           st.haven_months.as<int32_t>(), band_count, time_step_hours,
                           st.haven_longest.as<int32_t>(), st.haven_flags.as<uint8_t>(), out,
-                          sun->order);
+                          sun->order, earth->order);
         // The host month table must outlive its copy.
         LS_CUDA(cudaStreamSynchronize(ctx->stream));
     });

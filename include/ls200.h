@@ -224,7 +224,12 @@ ls200_status ls200_psr_run(ls200_context *ctx, const ls200_vectors *vectors, uin
  * [n,128,128], host geo_transforms/projections [n,6] f64, host windows
  * [n,4] (tile_x, tile_y, valid_width, valid_height), device horizons
  * [n,128,128,1440], device frames scratch [n,16384,12] f32, device out
- * [n, time_count, 128*128] (PSR, signal 3: [n, 128*128] over all vectors). */
+ * [n, time_count, 128*128] (PSR, signal 3: [n, 128*128] over all vectors).
+ * Steps are evaluated in the table's longitude order (outputs stay in time
+ * order).  A launch over part of the table first writes that part of the
+ * order into a buffer the table owns, so launches on one table that may run
+ * at the same time on different streams race on it; on the context's own
+ * stream they are ordered. */
 ls200_status ls200_lighting_device(ls200_context *ctx, int tile_count, const float *patch_dems,
                                    const double *geo_transforms, const double *projections,
                                    const int32_t *windows, const float *horizons,

@@ -121,9 +121,6 @@ __device__ __forceinline__ void body_direction(const Frame32 &f, float vx, float
     azimuth_deg = __fmul_rn(azimuth, kRadToDeg);
 }
 
-// Body-centre elevation minus the horizon interpolated at its azimuth
-// (lightmap_cpu.py:121-141).
-//
 // The signals read the horizon bins left, left+1, ... (wrapped at 1440)
 // through a bin accessor: GlobalBins reads the pixel's row, SharedBins a
 // window of it staged in shared memory.  Both return the same values.
@@ -155,6 +152,8 @@ __device__ __forceinline__ BinPosition margin_position(float azimuth_deg) {
     return BinPosition{left, fraction};
 }
 
+// Body-centre elevation minus the horizon interpolated at its azimuth
+// (lightmap_cpu.py:121-141).
 template <class Bins>
 __device__ __forceinline__ float horizon_margin_bins(const Bins &bin, float fraction,
                                                      float elevation) {

@@ -44,6 +44,30 @@ def test_python_binding_covers_every_declared_symbol():
     assert set(declared_functions()) <= set(_native.SIGNATURES)
 
 
+def declared_arities() -> dict[str, int]:
+    """Parameter count of every declaration in include/*.h."""
+    arities = {}
+    for header in HEADERS:
+        text = re.sub(r"/\*.*?\*/", "", header.read_text(), flags=re.S)
+        for name, params in re.findall(
+                r"\b(?:ls200_status|int|const char \*)\s*(ls200_\w+)\s*\(([^;]*?)\)\s*;", text,
+                flags=re.S):
+            params = params.strip()
+            arities[name] = 0 if params in ("", "void") else params.count(",") + 1
+    return arities
+
+
+def test_python_argument_lists_match_the_header():
+    from lunarscout_b200 import _native
+
+    arities = declared_arities()
+    assert set(arities) == set(declared_functions())
+    mismatched = {name: (count, len(_native.SIGNATURES[name]))
+                  for name, count in arities.items()
+                  if len(_native.SIGNATURES[name]) != count}
+    assert not mismatched, mismatched
+
+
 def test_import_does_not_initialise_cuda():
     code = (
         "import sys; sys.path.insert(0, %r)\n"

@@ -162,7 +162,11 @@ typedef struct ls200_site_tile {
  * azimuth) ray through all of its tile's DEM passes with work stealing.
  * traversal 0: the reference traversal, bit-identical to ls200_march_all_passes;
  * traversal 1: the skip ladder (a cull extends to the largest culled ancestor
- * cell, from 1 km on).  `device_out` holds tile_count x 16384 x azimuth_count
+ * cell, from 1 km on); traversals 2 and 3: 0 and 1 in the relative FP32
+ * arithmetic (positions as an integer origin plus small offsets, level-0
+ * heights relative to the observer's z, no rounded R + height), which stays
+ * within ~1e-4 deg of the FP64 restatement of the march where the reference
+ * arithmetic is off by up to ~0.02 deg at near-field samples.  `device_out` holds tile_count x 16384 x azimuth_count
  * floats, pixel-major per tile: slopes, or degrees when `degrees` (-inf kept
  * outside the primary DEM).  `seconds` (may be NULL) gets
  * {segments + setup, march}. */
@@ -246,6 +250,11 @@ ls200_status ls200_lighting_device(ls200_context *ctx, int tile_count, const flo
  * address and uploads the disk constants; make it before any stream capture.
  * All calls share the array: calls that overlap on the GPU (two streams, two
  * contexts on one device) race on it.  Nothing in it needs to start at zero.
+ * The array's address is cached per device index; after cudaDeviceReset the
+ * library must be reloaded before this entry point is called again.  It takes
+ * the table as plain vectors with no longitude order, so it evaluates steps in
+ * time order: the same products as ls200_lighting_device, but slower on long
+ * tables (a year hourly: about 0.4x its throughput).
  * Runs asynchronously on the context's stream. */
 ls200_status ls200_lighting_device_noalloc(ls200_context *ctx, int tile_count,
                                            const float *patch_dems,

@@ -18,9 +18,13 @@
 
 namespace ls200 {
 
+// Whether the disk constants are on a device yet.  Contexts on one device
+// each hold only their own lock, so the flag has a lock of its own.
+static std::mutex g_constants_lock;
 static bool g_constants_ready[64] = {};
 
 void ensure_lighting_constants(ls200_context *ctx) {
+    std::lock_guard<std::mutex> hold(g_constants_lock);
     if (g_constants_ready[ctx->device]) return;
     // Half-chords of a 16-column disk of radius float32(0.27) deg
     // (lightmap.py:19-25), rounded once to float32; the normaliser is twice

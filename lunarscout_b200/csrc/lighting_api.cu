@@ -153,7 +153,8 @@ ls200_status ls200_lighting_run(ls200_context *ctx, const ls200_vectors *vectors
     return guard([&] {
         LS_REQUIRE(ctx && vectors && out, "NULL argument");
         LS_REQUIRE(signal >= kSignalFraction && signal <= kSignalMargin, "unknown signal");
-        LS_REQUIRE(time_start >= 0 && time_count > 0 && time_start + time_count <= vectors->count,
+        LS_REQUIRE(time_start >= 0 && time_count > 0 &&
+                       int64_t(time_start) + time_count <= int64_t(vectors->count),
                    "time range outside the vector table");
         std::lock_guard<std::mutex> hold(ctx->lock);
         activate(ctx);
@@ -204,7 +205,8 @@ ls200_status ls200_lighting_device(ls200_context *ctx, int tile_count, const flo
         LS_REQUIRE(tile_count >= 1 && tile_count <= kMaxBatchTiles,
                    "tile_count must be between 1 and 32");
         LS_REQUIRE(signal >= kSignalFraction && signal <= kSignalPsr, "unknown signal");
-        LS_REQUIRE(time_start >= 0 && time_count > 0 && time_start + time_count <= vectors->count,
+        LS_REQUIRE(time_start >= 0 && time_count > 0 &&
+                       int64_t(time_start) + time_count <= int64_t(vectors->count),
                    "time range outside the vector table");
         std::lock_guard<std::mutex> hold(ctx->lock);
         activate(ctx);
@@ -522,7 +524,7 @@ ls200_status ls200_lighting_device_noalloc(ls200_context *ctx, int tile_count,
         LS_REQUIRE(vector_count > 0, "at least one vector is required");
         LS_REQUIRE(signal == kSignalPsr ||
                        (time_start >= 0 && time_count > 0 &&
-                        time_start + time_count <= vector_count),
+                        int64_t(time_start) + int64_t(time_count) <= int64_t(vector_count)),
                    "time range outside the vector table");
         std::lock_guard<std::mutex> hold(ctx->lock);
         activate(ctx);

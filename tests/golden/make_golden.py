@@ -1,7 +1,7 @@
 """Generate the committed golden fixtures under tests/golden/.
 
-Run on a machine that has the reference checkout (read-only) at
-REFERENCE_ROOT; the tests only read its outputs.  It imports the reference's own
+Run with LUNARSCOUT_REFERENCE set to the root of a lunarscout source checkout
+(read-only); the tests only read this script's outputs.  It imports the reference's own
 Python modules through a stub package (its top-level ``__init__`` needs
 pyproj/rasterio, absent here) and extracts:
 
@@ -20,7 +20,7 @@ pyproj/rasterio, absent here) and extracts:
   helpers on the reference CPU backend's lighting streams and on seeded
   synthetic streams (safe_haven_reference below).
 
-Usage: python tests/golden/make_golden.py [--simulate]
+Usage: LUNARSCOUT_REFERENCE=<checkout> python tests/golden/make_golden.py [--simulate]
 (--simulate re-runs the simulator capture, ~5 min).
 """
 
@@ -36,7 +36,9 @@ from pathlib import Path
 
 import numpy as np
 
-REFERENCE_ROOT = Path(os.environ.get("LUNARSCOUT_REFERENCE", "/root/reference"))
+if not os.environ.get("LUNARSCOUT_REFERENCE"):
+    sys.exit("set LUNARSCOUT_REFERENCE to the root of a lunarscout source checkout")
+REFERENCE_ROOT = Path(os.environ["LUNARSCOUT_REFERENCE"])
 PACKAGE = REFERENCE_ROOT / "src" / "lunarscout"
 DATA = REFERENCE_ROOT / "tests" / "data" / "numba_horizon"
 OUT = Path(__file__).resolve().parent

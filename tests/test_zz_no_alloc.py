@@ -75,11 +75,14 @@ def test_no_alloc_entry_point_matches_the_allocating_one_on_consecutive_calls(in
         table = DeviceVectors(context.handle, inputs["host_vectors"])
         count = len(inputs["host_vectors"])
         frames = torch.empty(TILES * PLANE * 12, dtype=torch.float32, device="cuda")
+        # (time start, time count, signal, output type); signal 3 (PSR) runs
+        # over the whole table and writes one plane per tile.
         calls = [(0, 40, 0, torch.float32), (40, count - 40, 1, torch.uint8),
-                 (5, 64, 2, torch.float32)]
+                 (5, 64, 2, torch.float32), (0, count, 3, torch.uint8)]
         for start, length, signal, dtype in calls:
-            expected = torch.full((TILES, length, PLANE), 7, dtype=dtype, device="cuda")
-            got = torch.full((TILES, length, PLANE), 9, dtype=dtype, device="cuda")
+            shape = (TILES, PLANE) if signal == 3 else (TILES, length, PLANE)
+            expected = torch.full(shape, 7, dtype=dtype, device="cuda")
+            got = torch.full(shape, 9, dtype=dtype, device="cuda")
             torch.cuda.synchronize()
             _native.check(lib.ls200_lighting_device(
                 context.handle, TILES, ctypes.c_void_p(inputs["patches"].data_ptr()),
@@ -98,6 +101,42 @@ def test_no_alloc_entry_point_matches_the_allocating_one_on_consecutive_calls(in
             # fraction tolerance of the lighting tests.
             assert torch.equal(got, expected), (start, length, signal)
         table.close()
+    finally:
+        context.close()
+
+
+def test_no_alloc_entry_point_takes_no_device_memory(inputs):
+    """After a first call on the device (which loads the kernels and looks up
+    the scratch address), further calls leave the device's free memory as it
+    was."""
+    import torch
+
+    from lunarscout_b200 import _native
+    from lunarscout_b200.lightmap_cuda import LightingContext
+
+    lib = _native.library()
+    context = LightingContext(0)
+    try:
+        stream = torch.cuda.current_stream()
+        _native.call("ls200_set_stream", context.handle, ctypes.c_void_p(stream.cuda_stream))
+        count = len(inputs["host_vectors"])
+        out = torch.empty((TILES, count, PLANE), dtype=torch.uint8, device="cuda")
+
+        def run():
+            _native.check(lib.ls200_lighting_device_noalloc(
+                context.handle, TILES, ctypes.c_void_p(inputs["patches"].data_ptr()),
+                inputs["geo"].ctypes.data, inputs["proj"].ctypes.data,
+                inputs["windows"].ctypes.data, ctypes.c_void_p(inputs["horizons"].data_ptr()),
+                ctypes.c_void_p(inputs["vectors"].data_ptr()), count, 0, count, 1,
+                ctypes.c_void_p(out.data_ptr())))
+            torch.cuda.synchronize()
+
+        run()
+        free_before, _ = torch.cuda.mem_get_info(0)
+        run()
+        run()
+        free_after, _ = torch.cuda.mem_get_info(0)
+        assert free_after == free_before
     finally:
         context.close()
 

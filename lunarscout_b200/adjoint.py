@@ -48,8 +48,8 @@ class SunLossProblem:
 
         from .lightmap_cuda import DeviceVectors
 
-        if traversal not in TRAVERSALS:
-            raise ValueError(f"traversal must be one of {sorted(TRAVERSALS)}")
+        if traversal not in ("exact", "ladder"):
+            raise ValueError("traversal must be 'exact' or 'ladder'")
         self.session = session
         self.maximum_distance_m = float(maximum_distance_m)
         self.observer_elevation_m = float(observer_elevation_m)

@@ -380,6 +380,7 @@ extern "C" ls200_status ls200_sun_loss_forward(ls200_context *ctx, const ls200_s
         LS_REQUIRE(tile_count >= 1 && tile_count <= kMaxBatchTiles,
                    "1 to 32 tiles per adjoint problem");
         LS_REQUIRE(azimuth_count >= 4, "azimuth_count must be at least 4");
+        LS_REQUIRE(traversal == 0 || traversal == 1, "the adjoint's traversal must be 0 or 1");
         LS_REQUIRE(disk_radius_deg > 0.0 && disk_radius_deg < 10.0,
                    "disk radius must be in (0, 10) degrees");
         LS_REQUIRE(sun->ctx == ctx && sun->count > 0, "sun vectors belong to another context");

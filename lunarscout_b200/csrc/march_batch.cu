@@ -143,7 +143,7 @@ __global__ void __launch_bounds__(128, kMinBlocks)
             const BatchDem &dem = P.dems[tile.dems[d]];
             const DemView view = dem.view;
             const float ratio = __fdiv_rn(primary.view.column_res, view.column_res);
-            const RaySegment g = interpolate_segment(
+            const RaySegment g = interpolate_segment<(kLadder & kRelative) != 0>(
                 tile.segments, P.center_count, tile.dem_count, d, azimuth, column, row,
                 tile.tile_column, tile.tile_row, kTileSide, P.subpatch, primary_width,
                 primary_height, ratio);
@@ -178,8 +178,12 @@ static void launch_sites(ls200_context *ctx, const SitesParams &P) {
 
 template <bool kCount, int kMinBlocks>
 static void dispatch(ls200_context *ctx, const SitesParams &P, int traversal) {
-    if (traversal == kReference) launch_sites<kCount, kReference, kMinBlocks>(ctx, P);
-    else launch_sites<kCount, kLadderClimb, kMinBlocks>(ctx, P);
+    switch (traversal) {
+        case kReference: launch_sites<kCount, kReference, kMinBlocks>(ctx, P); break;
+        case kLadderClimb: launch_sites<kCount, kLadderClimb, kMinBlocks>(ctx, P); break;
+        case kRelative: launch_sites<kCount, kRelative, kMinBlocks>(ctx, P); break;
+        default: launch_sites<kCount, kLadderClimb | kRelative, kMinBlocks>(ctx, P); break;
+    }
 }
 
 // The checkpointing march runs 8 blocks per SM too: its extra tracker
@@ -200,8 +204,8 @@ void march_sites_run(ls200_context *ctx, const ls200_site_tile *tiles, int tile_
     {
         LS_REQUIRE(ctx && tiles && device_out, "NULL argument");
         LS_REQUIRE(tile_count > 0, "tile_count must be positive");
-        LS_REQUIRE(traversal == kReference || traversal == kLadderClimb,
-                   "traversal must be 0 or 1");
+        LS_REQUIRE(traversal >= 0 && traversal <= (kLadderClimb | kRelative),
+                   "traversal must be 0 to 3");
         LS_REQUIRE(azimuth_count > 0 && static_cast<int64_t>(kTilePixels) * azimuth_count <
                                             (int64_t(1) << 31),
                    "azimuth_count is out of range");

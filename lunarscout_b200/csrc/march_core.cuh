@@ -30,6 +30,16 @@
 //
 // The skip ladder (kLadder, the batched traversal; no reference counterpart)
 // extends a cull to the largest culled ancestor cell, see ladder_advance.
+//
+// The relative arithmetic (kRelative; no reference counterpart) marches the
+// same algorithm in FP32 on coordinates and heights relative to a local
+// origin: positions as an integer origin (near the ray start) plus small
+// offsets, level-0 heights as differences from the observer's z taken
+// before interpolation, and the far-field local z from that difference
+// (never rounding R + height on its own).  The FP32 reference arithmetic
+// rounds absolute coordinates (an ulp of 5e-4 px at 4096 px) and absolute
+// heights, which at the 1 m first sample moves the slope by up to ~0.02 deg;
+// the relative march stays within ~1e-4 deg of the FP64 restatement.
 #pragma once
 
 #include "internal.cuh"
@@ -148,6 +158,70 @@ __device__ __forceinline__ float bilinear(const float *__restrict__ cells, int w
     return __fmaf_rn(ty, __fsub_rn(bottom, top), top);
 }
 
+// The relative arithmetic's level-0 sample: the height above `base` (the
+// observer's z) at column origin_x + offset_x, row origin_y + offset_y.  The
+// rounded absolute coordinates only decide the clamp; inside the clamp range
+// the cell comes from the origin plus the offset's integer part and the
+// fraction from the offset, and the corners are taken relative to `base`
+// before they are interpolated.  Returns false (no data) when a corner is
+// invalid.
+__device__ __forceinline__ bool bilinear_above(const float *__restrict__ cells, int width,
+                                               int height, int origin_x, float offset_x,
+                                               float absolute_x, int origin_y, float offset_y,
+                                               float absolute_y, float base, float &above) {
+    const float cmax = __fsub_rn(static_cast<float>(width), 1.0001f);
+    const float rmax = __fsub_rn(static_cast<float>(height), 1.0001f);
+    int x0, y0;
+    float tx, ty;
+    if (absolute_x >= 0.0f && absolute_x <= cmax && absolute_y >= 0.0f && absolute_y <= rmax) {
+        const float fx = floorf(offset_x), fy = floorf(offset_y);
+        x0 = origin_x + static_cast<int>(fx);
+        y0 = origin_y + static_cast<int>(fy);
+        tx = __fsub_rn(offset_x, fx);
+        ty = __fsub_rn(offset_y, fy);
+    } else {
+        float column = absolute_x > 0.0f ? absolute_x : 0.0f;
+        column = column < cmax ? column : cmax;
+        float row = absolute_y > 0.0f ? absolute_y : 0.0f;
+        row = row < rmax ? row : rmax;
+        x0 = static_cast<int>(floorf(column));
+        y0 = static_cast<int>(floorf(row));
+        tx = __fsub_rn(column, static_cast<float>(x0));
+        ty = __fsub_rn(row, static_cast<float>(y0));
+    }
+    const int x1 = min(x0 + 1, width - 1);
+    const int y1 = min(y0 + 1, height - 1);
+    const float *r0 = cells + static_cast<size_t>(y0) * width;
+    const float *r1 = cells + static_cast<size_t>(y1) * width;
+    float q00 = __ldg(r0 + x0), q10 = __ldg(r0 + x1);
+    float q01 = __ldg(r1 + x0), q11 = __ldg(r1 + x1);
+    if (!(q00 > -20000.0f && q10 > -20000.0f && q01 > -20000.0f && q11 > -20000.0f))
+        return false;
+    q00 = __fsub_rn(q00, base);
+    q10 = __fsub_rn(q10, base);
+    q01 = __fsub_rn(q01, base);
+    q11 = __fsub_rn(q11, base);
+    const float top = __fmaf_rn(tx, __fsub_rn(q10, q00), q00);
+    const float bottom = __fmaf_rn(tx, __fsub_rn(q11, q01), q01);
+    above = __fmaf_rn(ty, __fsub_rn(bottom, top), top);
+    return true;
+}
+
+// The relative arithmetic's far-field slope of a sample `above` metres above
+// the observer's z: the four-cell bound's local-z formula (bound_slope) with
+// the height difference given directly.
+__device__ __forceinline__ float above_slope(float dist, float above, float radius,
+                                             float observer_z, float observer_radius) {
+    const float squared = __fmul_rn(dist, dist);
+    float radius_sum = __fadd_rn(__fmul_rn(2.0f, radius), __fadd_rn(observer_z, above));
+    radius_sum = __fadd_rn(radius_sum, observer_z);
+    const float numerator = __fmaf_rn(above, radius_sum, -squared);
+    const float local_z = __fdiv_rn(numerator, __fmul_rn(2.0f, observer_radius));
+    const float lx2 = __fmaf_rn(dist, dist, -__fmul_rn(local_z, local_z));
+    const float local_x = lx2 > 0.0f ? __fsqrt_rn(lx2) : 1e-6f;
+    return __fdiv_rn(local_z, local_x);
+}
+
 // Local-z slope of a terrain point seen over the chord `dist`
 // (cuda_backend.py:812-830): numerator fused on its first product, local_x^2
 // fused on dist*dist.
@@ -254,15 +328,18 @@ __device__ __forceinline__ float cell_bound(const float *__restrict__ bounds, in
 // (min_x - px) <= 0 < (max_x - px), so the product with inv_x keeps that
 // order's sign pattern and the larger t is the edge ahead of the ray
 // (bitwise the same value, including the -0.0 of a ray starting on the edge).
-__device__ __forceinline__ float cell_exit_advance(int shift, int cx, int cy, float px, float py,
-                                                   float inv_x, float inv_y, float fallback) {
+// (ux, uy) is the position relative to the integer origin (origin_x,
+// origin_y); the reference arithmetic is origin 0 with u the absolute position.
+__device__ __forceinline__ float cell_exit_advance(int shift, int cx, int cy, float ux, float uy,
+                                                   int origin_x, int origin_y, float inv_x,
+                                                   float inv_y, float fallback) {
     const float scale_f = power_of_two(shift);
-    const float min_x = static_cast<float>(cx << shift);
-    const float min_y = static_cast<float>(cy << shift);
+    const float min_x = static_cast<float>((cx << shift) - origin_x);
+    const float min_y = static_cast<float>((cy << shift) - origin_y);
     const float edge_x = inv_x > 0.0f ? __fadd_rn(min_x, scale_f) : min_x;
     const float edge_y = inv_y > 0.0f ? __fadd_rn(min_y, scale_f) : min_y;
-    const float tmx = __fmul_rn(__fsub_rn(edge_x, px), inv_x);
-    const float tmy = __fmul_rn(__fsub_rn(edge_y, py), inv_y);
+    const float tmx = __fmul_rn(__fsub_rn(edge_x, ux), inv_x);
+    const float tmy = __fmul_rn(__fsub_rn(edge_y, uy), inv_y);
     const float exit_distance = tmx < tmy ? tmx : tmy;
     const float to_exit = exit_distance > 0.0f ? exit_distance : fallback;
     return to_exit > 0.0f ? __fadd_rn(to_exit, 0.0001f) : fallback;
@@ -290,7 +367,8 @@ __device__ __forceinline__ float cell_exit_advance(int shift, int cx, int cy, fl
 // `reached` to the largest culled level (`level` if none).
 template <class Table>
 __device__ __forceinline__ bool ladder_culled(const Table &table, const float *__restrict__ bounds,
-                                              int m, int ipx, int ipy, float px, float py,
+                                              int m, int ipx, int ipy, float ux, float uy,
+                                              int origin_x, int origin_y,
                                               float inv_x, float inv_y, bool near, float true_m,
                                               float radius, float observer_z,
                                               float observer_radius, float inverse_denominator,
@@ -299,7 +377,8 @@ __device__ __forceinline__ bool ladder_culled(const Table &table, const float *_
     const int cx = ipx >> shift, cy = ipy >> shift;
     const int4 L = table.cells(m);
     const float maximum_height = cell_bound(bounds, L, cx, cy);
-    step = cell_exit_advance(shift, cx, cy, px, py, inv_x, inv_y, __int_as_float(L.w));
+    step = cell_exit_advance(shift, cx, cy, ux, uy, origin_x, origin_y, inv_x, inv_y,
+                             __int_as_float(L.w));
     if (maximum_height < -20000.0f) return true;
     const float dh = __fsub_rn(maximum_height, observer_z);
     const float far_distance = __fadd_rn(__fadd_rn(true_m, __fmul_rn(step, 1010.0f)), 1.0f);
@@ -339,8 +418,9 @@ __device__ __forceinline__ bool ladder_culled(const Table &table, const float *_
 
 template <bool kCount, class Table>
 __device__ __forceinline__ float ladder_advance(const Table &table, const float *__restrict__ bounds,
-                                                int level, int top, int ipx, int ipy, float px,
-                                                float py, float inv_x, float inv_y, bool near,
+                                                int level, int top, int ipx, int ipy, float ux,
+                                                float uy, int origin_x, int origin_y,
+                                                float inv_x, float inv_y, bool near,
                                                 float true_m, float radius, float observer_z,
                                                 float observer_radius, float inverse_denominator,
                                                 float current, float advance, unsigned &visits,
@@ -351,8 +431,9 @@ __device__ __forceinline__ float ladder_advance(const Table &table, const float 
     for (int m = level + 1; m <= top; ++m) {
         float step;
         if (kCount) ++visits;
-        if (!ladder_culled(table, bounds, m, ipx, ipy, px, py, inv_x, inv_y, near, true_m, radius,
-                           observer_z, observer_radius, inverse_denominator, current, step))
+        if (!ladder_culled(table, bounds, m, ipx, ipy, ux, uy, origin_x, origin_y, inv_x, inv_y,
+                           near, true_m, radius, observer_z, observer_radius,
+                           inverse_denominator, current, step))
             break;
         best = step;
         reached = m;
@@ -361,13 +442,20 @@ __device__ __forceinline__ float ladder_advance(const Table &table, const float 
 }
 
 // One interpolated segment (fields 0,1,4..17 of the reference layout).
+// With the relative arithmetic start_x, start_y are relative to the integer
+// origin (origin_x, origin_y); otherwise the origin is 0.
 struct RaySegment {
     float start_x, start_y, a1, a2, a3, a4, b1, b2, b3, b4;
     float s_start, s_end, s_start_chord, c1, c2, c3;
+    int origin_x, origin_y;
 };
 
 // Subpatch interpolation of one ray's segment (cuda_backend.py:1032-1119):
 // four centres around the pixel, their start points shifted to the pixel.
+// kRelative: the origin is the integer part of the upper-left centre's start,
+// and the four starts are taken relative to it before the shift and the
+// interpolation (exact: they lie within a few pixels of each other).
+template <bool kRelative = false>
 __device__ __forceinline__ RaySegment interpolate_segment(
     const float *__restrict__ segments, int center_count, int dem_count, int pass_index,
     int azimuth, int column, int row, int tile_column, int tile_row, int tile_width,
@@ -403,11 +491,23 @@ __device__ __forceinline__ RaySegment interpolate_segment(
     const float *s00 = base + i00 * stride_c, *s10 = base + i10 * stride_c;
     const float *s01 = base + i01 * stride_c, *s11 = base + i11 * stride_c;
     float seg[kMarchFields];
+    int origin[2] = {0, 0};
+    if (kRelative) {
+        origin[0] = static_cast<int>(floorf(__ldg(s00 + 0)));
+        origin[1] = static_cast<int>(floorf(__ldg(s00 + 1)));
+    }
 #pragma unroll
     for (int k = 0; k < kMarchFields; ++k) {
         const int f = k < 2 ? k : k + 2;
         float v00 = __ldg(s00 + f), v10 = __ldg(s10 + f);
         float v01 = __ldg(s01 + f), v11 = __ldg(s11 + f);
+        if (kRelative && f < 2) {
+            const float o = static_cast<float>(origin[f]);
+            v00 = __fsub_rn(v00, o);
+            v10 = __fsub_rn(v10, o);
+            v01 = __fsub_rn(v01, o);
+            v11 = __fsub_rn(v11, o);
+        }
         if (f == 0) {
             v00 = __fmaf_rn(d_left, ratio, v00);
             v10 = __fmaf_rn(d_right, ratio, v10);
@@ -423,8 +523,9 @@ __device__ __forceinline__ RaySegment interpolate_segment(
         const float lower = __fmaf_rn(__fsub_rn(v11, v01), tx, v01);
         seg[k] = __fmaf_rn(__fsub_rn(lower, upper), ty, upper);
     }
-    return RaySegment{seg[0], seg[1], seg[2],  seg[3],  seg[4],  seg[5],  seg[6],  seg[7],
-                      seg[8], seg[9], seg[10], seg[11], seg[12], seg[13], seg[14], seg[15]};
+    return RaySegment{seg[0],  seg[1],  seg[2],  seg[3],  seg[4],    seg[5],   seg[6],
+                      seg[7],  seg[8],  seg[9],  seg[10], seg[11],   seg[12],  seg[13],
+                      seg[14], seg[15], origin[0], origin[1]};
 }
 
 // The state of one ray within one DEM pass of hierarchy_maximum.
@@ -445,8 +546,9 @@ __device__ __forceinline__ MarchState begin_pass(const DemView &dem, const RaySe
                       __int_as_float(0x7fffffff), INFINITY};
 }
 
-// Traversals of march_step: the reference's, and the skip ladder.
-enum Traversal { kReference = 0, kLadderClimb = 1 };
+// Traversals of march_step, a bit set: the reference's (0), the skip ladder
+// (bit 0) and the relative arithmetic (bit 1).
+enum Traversal { kReference = 0, kLadderClimb = 1, kRelative = 2 };
 
 // Which level-0 sample set the running maximum: nothing (NoArgmax, the
 // production kernels) or its position, distance and slope (Argmax, the
@@ -493,16 +595,36 @@ __device__ __forceinline__ bool march_step_tracked(const Table &table, const Dem
     float current = st.current;
     int level_hint = st.level_hint;
     float side_up = st.side_up, side_here = st.side_here;
+    constexpr bool relative = (kLadder & kRelative) != 0;
     if (!(s <= g.s_end)) return false;
     {
         if (kCount) ++steps;
         const float delta = __fsub_rn(s, g.s_start);
-        const float px = quartic(g.start_x, g.a1, g.a2, g.a3, g.a4, delta);
-        const float py = quartic(g.start_y, g.b1, g.b2, g.b3, g.b4, delta);
+        // Relative arithmetic: offsets along the ray without the start, added
+        // to the start relative to the origin; the absolute position (origin
+        // + offset, rounded) only takes the bounds decisions.
+        float rx, ry, ux, uy, px, py;
+        if (relative) {
+            rx = quartic(0.0f, g.a1, g.a2, g.a3, g.a4, delta);
+            ry = quartic(0.0f, g.b1, g.b2, g.b3, g.b4, delta);
+            ux = __fadd_rn(g.start_x, rx);
+            uy = __fadd_rn(g.start_y, ry);
+            px = __fadd_rn(static_cast<float>(g.origin_x), ux);
+            py = __fadd_rn(static_cast<float>(g.origin_y), uy);
+        } else {
+            px = quartic(g.start_x, g.a1, g.a2, g.a3, g.a4, delta);
+            py = quartic(g.start_y, g.b1, g.b2, g.b3, g.b4, delta);
+            ux = px;
+            uy = py;
+        }
         // NaN fails every comparison, as the reference's isnan tests do.
         if (!(px >= 0.0f && py >= 0.0f && px < last_x && py < last_y)) return false;
-        const float planar_x = __fmul_rn(__fsub_rn(px, g.start_x), resolution);
-        const float planar_y = __fmul_rn(__fsub_rn(py, g.start_y), resolution);
+        if (!relative) {
+            rx = __fsub_rn(px, g.start_x);
+            ry = __fsub_rn(py, g.start_y);
+        }
+        const float planar_x = __fmul_rn(rx, resolution);
+        const float planar_y = __fmul_rn(ry, resolution);
         const float planar_m = hypot_fused(planar_x, planar_y);
         const bool near = s < 0.5f;
         float true_m;
@@ -535,7 +657,10 @@ __device__ __forceinline__ bool march_step_tracked(const Table &table, const Dem
         const float dy = quartic_tangent(g.b1, g.b2, g.b3, g.b4, delta);
         const float inv_x = fabsf(dx) > 1e-8f ? __frcp_rn(dx) : 1e30f;
         const float inv_y = fabsf(dy) > 1e-8f ? __frcp_rn(dy) : 1e30f;
-        const int ipx = static_cast<int>(px), ipy = static_cast<int>(py);
+        const int origin_x = relative ? g.origin_x : 0;
+        const int origin_y = relative ? g.origin_y : 0;
+        const int ipx = relative ? origin_x + static_cast<int>(floorf(ux)) : static_cast<int>(px);
+        const int ipy = relative ? origin_y + static_cast<int>(floorf(uy)) : static_cast<int>(py);
         bool ray_out = false;
         for (;;) {
             const int4 L = table.cells(level);
@@ -548,8 +673,8 @@ __device__ __forceinline__ bool march_step_tracked(const Table &table, const Dem
                 break;
             }
             const float maximum_height = cell_bound(dem.bounds, L, cx, cy);
-            const float skip =
-                cell_exit_advance(shift, cx, cy, px, py, inv_x, inv_y, __int_as_float(L.w));
+            const float skip = cell_exit_advance(shift, cx, cy, ux, uy, origin_x, origin_y, inv_x,
+                                                 inv_y, __int_as_float(L.w));
             bool culled = maximum_height < -20000.0f;
             if (!culled) {
                 const float scale_f = power_of_two(shift);
@@ -560,27 +685,41 @@ __device__ __forceinline__ bool march_step_tracked(const Table &table, const Dem
             }
             if (culled) {
                 float advance = skip;
-                if (kLadder != kReference) {
+                if (kLadder & kLadderClimb) {
                     int reached;
                     advance = ladder_advance<kCount>(table, dem.bounds, level, top_level, ipx, ipy,
-                                                     px, py, inv_x, inv_y, near, true_m, radius,
-                                                     observer_z, observer_radius,
-                                                     inverse_denominator, current, skip, visits,
-                                                     reached);
+                                                     ux, uy, origin_x, origin_y, inv_x, inv_y,
+                                                     near, true_m, radius, observer_z,
+                                                     observer_radius, inverse_denominator,
+                                                     current, skip, visits, reached);
                 }
                 s = __fadd_rn(s, advance);
                 break;
             }
             if (level == 0) {
                 if (kCount) ++samples;
-                const float height = bilinear(cells, dem.width, dem.height, px, py);
                 float slope = -1e30f;
-                if (height > -20000.0f) {
-                    slope = near ? __fdiv_rn(__fsub_rn(height, observer_z), true_m)
-                                 : sample_slope(true_m, height, radius, observer_radius);
-                    if (slope > current) {
-                        current = slope;
-                        tracker.record(px, py, true_m, slope, near);
+                if (relative) {
+                    float above;
+                    if (bilinear_above(cells, dem.width, dem.height, origin_x, ux, px, origin_y,
+                                       uy, py, observer_z, above)) {
+                        slope = near ? __fdiv_rn(above, true_m)
+                                     : above_slope(true_m, above, radius, observer_z,
+                                                   observer_radius);
+                        if (slope > current) {
+                            current = slope;
+                            tracker.record(px, py, true_m, slope, near);
+                        }
+                    }
+                } else {
+                    const float height = bilinear(cells, dem.width, dem.height, px, py);
+                    if (height > -20000.0f) {
+                        slope = near ? __fdiv_rn(__fsub_rn(height, observer_z), true_m)
+                                     : sample_slope(true_m, height, radius, observer_radius);
+                        if (slope > current) {
+                            current = slope;
+                            tracker.record(px, py, true_m, slope, near);
+                        }
                     }
                 }
                 const float magnitude = hypot_fused(dx, dy);

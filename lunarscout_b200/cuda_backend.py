@@ -26,8 +26,11 @@ from .contract import PyramidArrays, map_parameters, projection_parameters
 __all__ = ["CudaBackendError", "CudaExecutionError", "CudaDeviceInfo", "CudaSession",
            "DeviceDem", "SiteTile", "BatchConfig", "TRAVERSALS"]
 
-#: Traversals of the batched march: the reference's, and the skip ladder.
-TRAVERSALS = {"exact": 0, "ladder": 1}
+#: Traversals of the batched march: the reference's ("exact", bit-identical to
+#: the drop-in), the skip ladder, and both in the relative FP32 arithmetic
+#: (coordinates and heights relative to a local origin; within ~1e-4 deg of
+#: the FP64 restatement of the march, not bit-identical to the reference).
+TRAVERSALS = {"exact": 0, "ladder": 1, "relative": 2, "relative-ladder": 3}
 
 # Slope arrays returned by the march calls live in recycled pinned memory
 # (fresh, ordinary numpy arrays to the caller).

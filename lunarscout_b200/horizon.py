@@ -483,15 +483,20 @@ def generate_horizons_from_grids(
     build_subpatch_segments_numba (the public path fixes 1,000 km).
     ``batch_tiles`` > 0 marches that many patches per persistent launch;
     ``traversal="ladder"`` (batched only) uses the skip ladder instead of the
-    reference traversal (not bit-identical to the reference's tiles)."""
+    reference traversal (not bit-identical to the reference's tiles);
+    ``"relative"`` / ``"relative-ladder"`` (batched only) march those
+    traversals in the relative FP32 arithmetic (closer to the FP64
+    restatement, not bit-identical to the reference's tiles)."""
     if not dems or not all(isinstance(dem, DemGrid) for dem in dems):
         raise InputError("dems must be a non-empty sequence of DemGrid, primary first.",
                          code="horizon_dem_paths_invalid")
     if isinstance(batch_tiles, bool) or not isinstance(batch_tiles, int) or batch_tiles < 0:
         raise InputError("batch_tiles must be a non-negative integer.",
                          code="horizon_option_invalid", details={"argument": "batch_tiles"})
-    if traversal not in ("exact", "ladder") or (traversal == "ladder" and batch_tiles == 0):
-        raise InputError("traversal must be 'exact', or 'ladder' with batch_tiles > 0.",
+    if (traversal not in ("exact", "ladder", "relative", "relative-ladder")
+            or (traversal != "exact" and batch_tiles == 0)):
+        raise InputError("traversal must be 'exact', or 'ladder', 'relative' or "
+                         "'relative-ladder' with batch_tiles > 0.",
                          code="horizon_option_invalid", details={"argument": "traversal"})
     if not (isinstance(maximum_distance_m, Real) and np.isfinite(maximum_distance_m)
             and maximum_distance_m > 0.0):

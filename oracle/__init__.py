@@ -63,6 +63,10 @@ OPT_EXIT_CAP = 1 << 16
 #: Skip ladder of the batched traversal (no reference counterpart): a cull
 #: climbs to the largest culled ancestor cell before skipping.
 OPT_LADDER = 1 << 20
+#: Relative-height level-0 slopes (this project's accuracy mode): local z from
+#: height - observer_z and 2R + height + observer_z, never from R + height
+#: rounded on its own.
+OPT_RELATIVE = 1 << 21
 
 
 def ladder_mask(cap: int = 0, min_km: int = 0, base: int | None = None) -> int:
@@ -131,6 +135,8 @@ def _declare(library: ctypes.CDLL) -> None:
     library.ora_march_pass_f64.restype = _c.c_int
     library.ora_march_trace_f32.argtypes = march_args + [_f32p, _c.c_uint, _f32p, _c.c_int]
     library.ora_march_trace_f32.restype = _c.c_int
+    library.ora_march_trace_f64.argtypes = march_args + [_f64p, _c.c_uint, _f32p, _c.c_int]
+    library.ora_march_trace_f64.restype = _c.c_int
     library.ora_hierarchy_maximum_f32.argtypes = [
         _f32p, _f32p, _c.c_int, _c.c_int, _f32p, _i32p, _c.c_int,
         _c.c_float, _c.c_float, _c.c_float, _c.c_int, _c.c_float, _c.c_uint,
@@ -299,17 +305,18 @@ def march_all_passes(
 def march_trace(
     segments, primary, active, *, tile_column, tile_row, tile_width, tile_height,
     subpatch_size, pass_index, pixel, azimuth, observer_elevation_m=0.0,
-    initial=-np.inf, mask=PRODUCTION_MASK, capacity=65536,
+    initial=-np.inf, mask=PRODUCTION_MASK, capacity=65536, precision="f32",
 ) -> tuple[float, np.ndarray]:
-    """One ray of one pass with its 12-field branch trace."""
+    """One ray of one pass with its 12-field branch trace (rows in float32)."""
     segments = np.ascontiguousarray(segments, dtype=np.float32)
     azimuth_count, center_count, dem_count, _ = segments.shape
     primary_level0 = np.ascontiguousarray(primary.level0, dtype=np.float32)
-    slope = np.array([initial], dtype=np.float32)
+    slope = np.array([initial], dtype=np.float32 if precision == "f32" else np.float64)
+    function = lib().ora_march_trace_f32 if precision == "f32" else lib().ora_march_trace_f64
     rows = np.zeros((capacity, 12), dtype=np.float32)
     pixels = np.array([pixel], dtype=np.int32)
     azimuths = np.array([azimuth], dtype=np.int32)
-    count = lib().ora_march_trace_f32(
+    count = function(
         segments, azimuth_count, center_count, dem_count,
         primary_level0, primary_level0.shape[1], primary_level0.shape[0],
         np.ascontiguousarray(primary.map_parameters, dtype=np.float32),

@@ -54,6 +54,11 @@ enum {
      * four-cell bound is culled too, and skip to the exit of the largest
      * culled cell.  Bits 24..27 cap the climb (0 = up to the top level). */
     ORA_OPT_LADDER = 1u << 20,
+    /* Relative-height level-0 slopes (this project's accuracy mode, not the
+     * reference's): the sample's local z is formed from height - observer_z
+     * and 2R + height + observer_z, as the four-cell bound's is, instead of
+     * from the rounded radii R + height and R + observer_z. */
+    ORA_OPT_RELATIVE = 1u << 21,
 };
 #define ORA_LADDER_CAP(mask) (((mask) >> 24) & 15u)
 /* Bits 28..31: the ladder acts only from this distance on, in km. */
@@ -222,6 +227,24 @@ int ora_march_trace_f32(ORA_MARCH_ARGS, float *slope_inout, unsigned mask,
     return trace.count;
 }
 
+/* The same in FP64 (the trace rows are stored as float32). */
+int ora_march_trace_f64(ORA_MARCH_ARGS, double *slope_inout, unsigned mask,
+                        float *trace_rows, int capacity)
+{
+    (void)n;
+    ora_pyramid primary, active;
+    make_pyramid(&primary, p_level0, p_width, p_height, NULL, NULL, 0, p_map, NULL);
+    make_pyramid(&active, a_level0, a_width, a_height, a_mips, a_levels, a_level_count,
+                 a_map, a_projection);
+    ora_trace trace = {trace_rows, capacity, 0};
+    (void)tile_height;
+    march_one_f64(segments, azimuth_count, center_count, dem_count, &primary, &active,
+                  tile_column, tile_row, tile_width, subpatch, pass_index,
+                  observer_elevation, pixels[0], azimuths[0], slope_inout, mask, NULL,
+                  &trace);
+    return trace.count;
+}
+
 /* The bare march of one already-interpolated 16-field segment
  * (start_x, start_y, a1..a4, b1..b4, s_start, s_end, s_start_chord, c1..c3). */
 float ora_hierarchy_maximum_f32(const float *segment16, const float *level0, int width,
@@ -237,7 +260,7 @@ float ora_hierarchy_maximum_f32(const float *segment16, const float *level0, int
     float seg[16];
     memcpy(seg, segment16, sizeof seg);
     float r = hierarchy_maximum_f32(seg, &p, observer_z, radius, resolution, pass_index,
-                                    initial, mask, NULL, trace_rows ? &trace : NULL);
+                                    initial, mask, NULL, trace_rows ? &trace : NULL, 0, 0);
     if (trace_count) *trace_count = trace.count;
     return r;
 }

@@ -88,11 +88,20 @@ def test_exact_traversal_equals_the_per_tile_path(batch, cuda_session):
     assert np.isneginf(got[1].reshape(128, 128, AZ)[:, 72:]).all()   # x >= 200 on site b
 
 
-def test_ladder_traversal_equals_its_cpu_restatement(batch, cuda_session):
+# The batched traversals and the oracle masks that restate them.
+CPU_MASKS = {
+    "ladder": oracle.ladder_mask(0, 1),
+    "relative": oracle.PRODUCTION_MASK | oracle.OPT_RELATIVE,
+    "relative-ladder": oracle.ladder_mask(0, 1) | oracle.OPT_RELATIVE,
+}
+
+
+@pytest.mark.parametrize("traversal", sorted(CPU_MASKS))
+def test_batched_traversal_equals_its_cpu_restatement(batch, cuda_session, traversal):
     from lunarscout_b200.contract import PyramidArrays, map_parameters, projection_parameters
 
     tiles, grids = batch
-    got = _run(cuda_session, tiles, "ladder")
+    got = _run(cuda_session, tiles, traversal)
     for t, tile in enumerate(tiles):
         dems = [grids[id(d)] for d in tile.dems]
         segments = cuda_session.generate_segments(
@@ -106,8 +115,7 @@ def test_ladder_traversal_equals_its_cpu_restatement(batch, cuda_session):
                                           projection_parameters(dem)))
         expected, _ = oracle.march_all_passes(
             segments, pyramids, tile_column=tile.tile_column, tile_row=tile.tile_row,
-            observer_elevation_m=tile.observer_elevation_m,
-            mask=oracle.ladder_mask(0, 1))
+            observer_elevation_m=tile.observer_elevation_m, mask=CPU_MASKS[traversal])
         np.testing.assert_array_equal(got[t], expected, err_msg=f"tile {t}")
 
 
@@ -160,7 +168,7 @@ def test_batch_validation(batch, cuda_session):
         cuda_session.march_sites([], device_out=out.data_ptr(), azimuth_count=AZ)
 
 
-@pytest.mark.parametrize("traversal", ["exact", "ladder"])
+@pytest.mark.parametrize("traversal", ["exact", "ladder", "relative-ladder"])
 def test_results_are_invariant_across_launch_configurations(batch, cuda_session, traversal):
     from lunarscout_b200.autotune import DEFAULT_CANDIDATES
 

@@ -179,68 +179,89 @@ def build_dems():
     return primary, regional
 
 
+class CpuMarchSample:
+    """The oracle's C restatement of the march (all host threads) on random
+    rays of one site-scale tile, both DEM passes: pyramids and segments are
+    built once, then each call marches a fresh random ray sample."""
+
+    def __init__(self, primary, regional, tile, threads=None):
+        import oracle
+        from oracle import segments as oseg
+        from lunarscout_b200.contract import PyramidArrays, map_parameters, projection_parameters
+
+        self.oracle = oracle
+        self.pyramids = []
+        for dem in (primary, regional):
+            mips, levels = oracle.build_pyramid(dem.elevation_m)
+            self.pyramids.append(PyramidArrays(dem.elevation_m, mips, levels,
+                                               map_parameters(dem), projection_parameters(dem)))
+        self.threads = threads or oracle.default_threads()
+        self.tile_row, self.tile_column = tile
+        self.segments = oseg.build_segments(
+            [primary, regional], tile_column=self.tile_column, tile_row=self.tile_row,
+            tile_width=TILE, azimuth_count=AZIMUTHS, maximum_distance_m=RANGE_M,
+            observer_elevation_m=OBSERVER_M, threads=self.threads)
+        self.rng = np.random.default_rng(7)
+
+    def run(self, rays: int) -> float:
+        """March `rays` random rays; returns the elapsed seconds."""
+        pixels = self.rng.integers(0, TILE * TILE, size=rays).astype(np.int32)
+        azimuths = self.rng.integers(0, AZIMUTHS, size=rays).astype(np.int32)
+        started = time.perf_counter()
+        self.oracle.march_all_passes(self.segments, self.pyramids, tile_column=self.tile_column,
+                                     tile_row=self.tile_row, observer_elevation_m=OBSERVER_M,
+                                     pixels=pixels, azimuths=azimuths, threads=self.threads)
+        return time.perf_counter() - started
+
+
 def cpu_sample_rate(primary, regional, tiles, seconds_target=12.0, threads=None):
     """Oracle march throughput (rays/s) on a bounded random ray sample."""
-    import oracle
-    from oracle import segments as oseg
-    from lunarscout_b200.contract import PyramidArrays, map_parameters, projection_parameters
-
-    pyramids = []
-    for dem in (primary, regional):
-        mips, levels = oracle.build_pyramid(dem.elevation_m)
-        pyramids.append(PyramidArrays(dem.elevation_m, mips, levels, map_parameters(dem),
-                                      projection_parameters(dem)))
-    threads = threads or oracle.default_threads()
-    tile_row, tile_column = tiles[0]
-    segments = oseg.build_segments([primary, regional], tile_column=tile_column,
-                                   tile_row=tile_row, tile_width=TILE, azimuth_count=AZIMUTHS,
-                                   maximum_distance_m=RANGE_M, observer_elevation_m=OBSERVER_M,
-                                   threads=threads)
-    rng = np.random.default_rng(7)
-    count = 256
-    elapsed = 0.0
-    rays = 0
+    sample = CpuMarchSample(primary, regional, tiles[0], threads)
+    count, elapsed, rays = 256, 0.0, 0
     while elapsed < seconds_target:
-        pixels = rng.integers(0, TILE * TILE, size=count).astype(np.int32)
-        azimuths = rng.integers(0, AZIMUTHS, size=count).astype(np.int32)
-        started = time.perf_counter()
-        oracle.march_all_passes(segments, pyramids, tile_column=tile_column, tile_row=tile_row,
-                                observer_elevation_m=OBSERVER_M, pixels=pixels,
-                                azimuths=azimuths, threads=threads)
-        took = time.perf_counter() - started
+        took = sample.run(count)
         elapsed += took
         rays += count
         if took < 1.0:
             count *= 4
-    return rays / elapsed, threads, rays, elapsed
+    return rays / elapsed, sample.threads, rays, elapsed
+
+
+# Rays of one reference-arm step: a bounded sample of the site-scale tile
+# (about a second of CPU work on a 16-core host).
+REFERENCE_STEP_RAYS = 1 << 17
 
 
 def run_reference(args):
+    """The reference algorithm on the host cores: each step marches a fresh
+    random sample of REFERENCE_STEP_RAYS rays of the site-scale tile (both DEM
+    passes) with the oracle's C restatement; value = rays / measured seconds
+    per step, ms_per_step = the measured step time (median)."""
     rank, world, _ = dist_env()
     if rank != 0:
         return
     primary, regional = build_dems()
-    tiles = tile_schedule(0, 1, 1)
+    sample = CpuMarchSample(primary, regional, tile_schedule(0, 1, 1)[0])
     per_step = []
-    rates = []
     for step in range(args.warmup + args.steps):
-        rate, threads, rays, elapsed = cpu_sample_rate(primary, regional, tiles,
-                                                       seconds_target=args.reference_seconds)
+        took = sample.run(REFERENCE_STEP_RAYS)
         if step >= args.warmup:
-            rates.append(rate)
-            per_step.append(elapsed)
-    value = statistics.median(rates)
+            per_step.append(took)
+    step_seconds = statistics.median(per_step)
+    value = REFERENCE_STEP_RAYS / step_seconds
     line = {
         "impl": "reference",
         "metric": METRIC, "value": value, "unit": "rays/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup,
-        "ms_per_step": 1000.0 * RAYS_PER_TILE / value,
+        "ms_per_step": 1000.0 * step_seconds,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic",
         "config": workload_config(),
-        "cpu_baseline": {"value": value, "unit": "rays/s", "cores": threads, "kind": "port",
-                         "sample": f"random rays of a site-scale tile, both DEM passes, "
-                                   f"~{args.reference_seconds:.0f} s of CPU work per step"},
+        "cpu_baseline": {"value": value, "unit": "rays/s", "cores": sample.threads,
+                         "kind": "port",
+                         "sample": f"each step: {REFERENCE_STEP_RAYS} random rays of a "
+                                   f"site-scale tile, both DEM passes (a step of the GPU arm "
+                                   f"is the whole tile, {RAYS_PER_TILE} rays)"},
         "e2e": {"value": value, "unit": "rays/s", "h2d_bytes_per_step": 0,
                 "d2h_bytes_per_step": 0},
     }
@@ -384,38 +405,114 @@ def lighting_benchmark(session, dems, segments, tiles, primary, args, world, ran
         "output_gbs": value / 1e9,
     }
     if rank == 0 and world == 1 and not args.skip_cpu:
-        import oracle  # noqa: F401  (CPU leg only)
-        from oracle import products
-
         host_horizons = horizons[0].cpu().numpy().reshape(TILE, TILE, AZIMUTHS)
         tile_row, tile_column = tiles[picks[0]]
-        sample = vectors.astype(np.float64)  # one tile, the whole year
-        started = time.perf_counter()
-        products.lighting_tiles(primary, host_horizons, sample, tile_y=tile_row,
-                                tile_x=tile_column)
-        took = time.perf_counter() - started
-        result["cpu_baseline"] = {
-            "value": plane * len(sample) / took, "unit": "px·steps/s",
-            "cores": products.default_threads(), "kind": "port",
-            "sample": f"one tile x {len(sample)} hourly steps ({took:.1f} s)"}
+        reference = reference_cpu_lighting(primary, host_horizons, tile_row, tile_column,
+                                           synthetic.sun_vectors(hours))
+        if reference is not None:
+            result["cpu_baseline"] = reference["lightmap"]
+            result["reference_cpu_psr"] = reference["psr"]
+        else:
+            from oracle import products
+
+            sample = vectors.astype(np.float64)  # one tile, the whole year
+            started = time.perf_counter()
+            products.lighting_tiles(primary, host_horizons, sample, tile_y=tile_row,
+                                    tile_x=tile_column)
+            took = time.perf_counter() - started
+            result["cpu_baseline"] = {
+                "value": plane * len(sample) / took, "unit": "px·steps/s",
+                "cores": products.default_threads(), "kind": "port",
+                "sample": f"one tile x {len(sample)} hourly steps ({took:.1f} s)"}
     return result
 
 
+def reference_cpu_lighting(primary, host_horizons, tile_row, tile_column, sun_vectors):
+    """The reference's own CPU lighting on the box's host cores:
+    LightmapCpuSession (lightmap_cpu.py:193, Numba parallel) sun-fraction
+    bytes of one tile over the year, and compute_psr_patch_reference
+    (psr.py:94, NumPy per pixel) on a 32 x 32 window against the reduced
+    vectors.  None when the reference is not installed."""
+    runtime = reference_runtime()
+    if runtime is None:
+        return None
+    import numba
+
+    runtime.import_reference()
+    from lunarscout._numba_horizon.lightmap_cpu import LightmapCpuSession
+    from lunarscout._numba_horizon.psr import (compute_psr_patch_reference,
+                                               reduce_sun_vectors_for_psr)
+
+    dem = reference_dem(primary)
+    horizons = np.where(np.isneginf(host_horizons), np.float32(-50.0), host_horizons)
+    session = LightmapCpuSession(time_batch_size=32)
+    tile = dict(tile_y=tile_row, tile_x=tile_column)
+    for _ in session.iter_patch_tiles(dem, horizons, sun_vectors[:64], **tile):
+        pass  # compiles the Numba kernels
+    started = time.perf_counter()
+    for _ in session.iter_patch_tiles(dem, horizons, sun_vectors, **tile):
+        pass
+    lightmap_s = time.perf_counter() - started
+    reduced, _ = reduce_sun_vectors_for_psr(dem, sun_vectors)
+    window = 32
+    started = time.perf_counter()
+    compute_psr_patch_reference(dem, horizons, reduced, valid_height=window,
+                                valid_width=window, **tile)
+    psr_s = time.perf_counter() - started
+    return {
+        "lightmap": {"value": TILE * TILE * len(sun_vectors) / lightmap_s, "unit": "px·steps/s",
+                     "cores": numba.config.NUMBA_NUM_THREADS, "kind": "reference",
+                     "sample": f"LightmapCpuSession.iter_patch_tiles, one tile x "
+                               f"{len(sun_vectors)} hourly steps ({lightmap_s:.1f} s)"},
+        "psr": {"value": window * window * len(reduced) / psr_s,
+                "unit": "px·reduced vectors/s", "cores": 1, "kind": "reference",
+                "sample": f"compute_psr_patch_reference, {window}x{window} px x "
+                          f"{len(reduced)} reduced vectors ({psr_s:.1f} s)"},
+    }
+
+
 SITES = 64
-SITE_TILES_PER_BATCH = 16
-SITE_BATCHES = 3  # one warm-up batch, then timed batches
+WARMUP_TILES = 16  # the warm-up batch: one tile of each of the first 16 sites
 TUNE_TILES = 4
-ACCURACY_RAYS_PER_TILE = 512
+MULTISITE_PARITY_RAYS = 20_000
+# The multi-site products run over this many of the batch's 64 tiles by
+# default (one lighting launch); --c3-full-lighting takes all 64.
+C3_LIGHT_TILES = 8
+
+
+def distance_over_every_ray(a, b, bin_deg=1e-5, bins=100_000):
+    """p99.9 (to the histogram's bin width) and max of |a - b| (degrees) over
+    every finite ray of two degree batches [tiles, pixels, azimuths]; returns
+    also whether the -inf rays agree."""
+    import torch
+
+    counts = torch.zeros(bins + 1, dtype=torch.int64, device=a.device)
+    largest, same_inf, total = 0.0, True, 0
+    for t in range(a.shape[0]):
+        finite = torch.isfinite(a[t])
+        same_inf &= bool(torch.equal(finite, torch.isfinite(b[t])))
+        d = (a[t].double() - b[t].double())[finite & torch.isfinite(b[t])].abs()
+        if d.numel() == 0:
+            continue
+        total += d.numel()
+        largest = max(largest, float(d.max()))
+        counts += torch.bincount((d / bin_deg).long().clamp(max=bins), minlength=bins + 1)
+    cumulative = torch.cumsum(counts, 0)
+    rank = int(math.ceil(0.999 * int(cumulative[-1])))
+    index = int(torch.searchsorted(cumulative, torch.tensor([rank], device=a.device)))
+    return {"p99.9": (index + 1) * bin_deg, "max": largest, "rays": total,
+            "inf_rays_agree": same_inf}
 
 
 def multisite_benchmark(session, stream, args, world, rank):
     """The uneven multi-site workload (64 sites, sides 256-2048 px at 5-40 m,
-    latitudes -83 to -89.5, one polar 240 m regional DEM, 200 km rays): each
-    batch is one tile from each of 16 sites.  Plain = per-tile device segments
-    + per-pass launches + transpose; batched = one persistent work-stealing
-    launch over the whole batch (reference traversal, then skip ladder), its
-    launch configuration chosen by the autotuner on part of the warm-up
-    batch.  All produce degrees in HBM and are timed with CUDA events."""
+    latitudes -83 to -89.5, one polar 240 m regional DEM, 200 km rays): the
+    timed batch is one tile of EVERY site (64 tiles) in one launch.  Plain =
+    per-tile device segments + per-pass launches + transpose; batched = one
+    persistent work-stealing launch over the whole batch (reference
+    traversal, skip ladder, and the ladder in the relative FP32 arithmetic),
+    launch configuration chosen by the autotuner.  Degrees in HBM, CUDA
+    events; a smaller warm-up batch precedes each timed one."""
     import torch
     import torch.distributed as dist
 
@@ -431,29 +528,30 @@ def multisite_benchmark(session, stream, args, world, rank):
     regional_dev = session.upload_dem_grid(regional)
     site_devs = [session.upload_dem_grid(grid) for grid in grids]
     rng = np.random.default_rng(77 + rank)
-    batches, picks = [], []
-    for b in range(SITE_BATCHES):
-        tiles, chosen = [], []
-        for j in range(SITE_TILES_PER_BATCH):
-            site = (rank * SITE_TILES_PER_BATCH * SITE_BATCHES + b * SITE_TILES_PER_BATCH + j) % SITES
-            grid = grids[site]
-            tx = int(rng.integers(0, (grid.width + TILE - 1) // TILE)) * TILE
-            ty = int(rng.integers(0, (grid.height + TILE - 1) // TILE)) * TILE
-            tiles.append(SiteTile((site_devs[site], regional_dev), tx, ty, RANGE_M, OBSERVER_M))
-            chosen.append(site)
-        batches.append(tiles)
-        picks.append(chosen)
-    timed_rays = sum(min(TILE, grids[s].width - t.tile_column)
-                     * min(TILE, grids[s].height - t.tile_row) * AZIMUTHS
-                     for tiles, chosen in zip(batches[1:], picks[1:])
-                     for t, s in zip(tiles, chosen))
+
+    def random_tile(site):
+        grid = grids[site]
+        tx = int(rng.integers(0, (grid.width + TILE - 1) // TILE)) * TILE
+        ty = int(rng.integers(0, (grid.height + TILE - 1) // TILE)) * TILE
+        return SiteTile((site_devs[site], regional_dev), tx, ty, RANGE_M, OBSERVER_M)
+
+    warmup = [random_tile(site) for site in range(WARMUP_TILES)]
+    batch = [random_tile(site) for site in range(SITES)]
+
+    def valid(tile, site):
+        grid = grids[site]
+        return (min(TILE, grid.width - tile.tile_column),
+                min(TILE, grid.height - tile.tile_row))
+
+    timed_rays = sum(w * h for w, h in (valid(t, s) for s, t in enumerate(batch))) * AZIMUTHS
     centers = (TILE // 8 + 2) ** 2
     segments = torch.empty(AZIMUTHS * centers * 2 * 18, dtype=torch.float32, device="cuda")
-    out = torch.empty((SITE_TILES_PER_BATCH, TILE * TILE, AZIMUTHS), dtype=torch.float32,
-                      device="cuda")
+    outputs = {name: torch.empty((SITES, TILE * TILE, AZIMUTHS), dtype=torch.float32,
+                                 device="cuda")
+               for name in ("exact", "ladder", "relative-ladder")}
     torch.cuda.synchronize()
 
-    def plain(tiles):
+    def plain(tiles, out):
         for i, tile in enumerate(tiles):
             dems = list(tile.dems)
             session.generate_segments_device(dems, segments.data_ptr(),
@@ -467,178 +565,80 @@ def multisite_benchmark(session, stream, args, world, rank):
                                             observer_elevation_m=OBSERVER_M,
                                             device_out=out[i].data_ptr(), degrees=True)
 
-    splits = {}  # traversal -> [(segment + setup seconds, march seconds)] per call
+    splits = {}  # traversal -> (segment + setup seconds, march seconds) of the timed call
 
     def batched(traversal):
-        def run(tiles):
-            splits.setdefault(traversal, []).append(session.march_sites(
+        def run(tiles, out):
+            splits[traversal] = session.march_sites(
                 tiles, device_out=out.data_ptr(), azimuth_count=AZIMUTHS, traversal=traversal,
-                degrees=True))
+                degrees=True)
         return run
 
-    def timed(run):
-        run(batches[0])
+    def timed(run, out):
+        run(warmup, out)
         torch.cuda.synchronize()
         if world > 1:
             dist.barrier()
         start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         start.record(stream)
-        for tiles in batches[1:]:
-            run(tiles)
+        run(batch, out)
         end.record(stream)
         torch.cuda.synchronize()
         elapsed = max_over_ranks(start.elapsed_time(end) / 1000.0, world)
         return world * timed_rays / elapsed, elapsed
 
-    tuned = tune_batch(session, batches[0][:TUNE_TILES], device_out=out.data_ptr(),
+    tuned = tune_batch(session, warmup[:TUNE_TILES], device_out=outputs["ladder"].data_ptr(),
                        azimuth_count=AZIMUTHS, traversal="ladder")
-    plain_value, plain_s = timed(plain)
-    exact_value, exact_s = timed(batched("exact"))
-    ladder_value, ladder_s = timed(batched("ladder"))
+    values, seconds = {}, {}
+    values["plain"], seconds["plain"] = timed(plain, outputs["exact"])
+    for traversal in ("exact", "ladder", "relative-ladder"):
+        values[traversal], seconds[traversal] = timed(batched(traversal), outputs[traversal])
     result = {
         "metric": "multi-site horizon rays/s (uneven batch, 2 DEM passes, 200 km)",
         "unit": "rays/s",
-        "plain_per_tile": plain_value,
-        "batched_exact": exact_value,
-        "batched_ladder": ladder_value,
-        "speedup_batched_vs_plain": ladder_value / plain_value,
-        "speedup_exact_vs_plain": exact_value / plain_value,
-        "seconds": {"plain": plain_s, "exact": exact_s, "ladder": ladder_s},
+        "plain_per_tile": values["plain"],
+        "batched_exact": values["exact"],
+        "batched_ladder": values["ladder"],
+        "batched_relative_ladder": values["relative-ladder"],
+        "speedup_batched_vs_plain": values["ladder"] / values["plain"],
+        "speedup_relative_ladder_vs_plain": values["relative-ladder"] / values["plain"],
+        "speedup_exact_vs_plain": values["exact"] / values["plain"],
+        "seconds": seconds,
         "batched_split_seconds": {
-            traversal: {"segments_and_setup": sum(s for s, _ in calls[-(SITE_BATCHES - 1):]),
-                        "march": sum(m for _, m in calls[-(SITE_BATCHES - 1):])}
-            for traversal, calls in splits.items()},
+            traversal: {"segments_and_setup": split[0], "march": split[1]}
+            for traversal, split in splits.items()},
         "launch_config": {"lanes_per_azimuth": tuned.best.lanes_per_azimuth,
                           "min_blocks": tuned.best.min_blocks,
                           "tuned_on": f"{TUNE_TILES} tiles of the warm-up batch, ladder",
                           "candidates_ms": {
                               f"lanes{c.lanes_per_azimuth}/blocks{c.min_blocks}":
                                   1000.0 * s for c, s in tuned.seconds.items()}},
-        "sites": SITES, "tiles_per_batch": SITE_TILES_PER_BATCH,
-        "timed_batches": SITE_BATCHES - 1, "rays_timed_per_rank": timed_rays,
+        "sites": SITES, "tiles_per_launch": SITES, "warmup_tiles": WARMUP_TILES,
+        "rays_timed_per_rank": timed_rays,
         "rays": "rays of pixels inside each site DEM (partial edge tiles count their valid part)",
+        "every_ray_vs_exact_deg": {
+            "ladder": distance_over_every_ray(outputs["ladder"], outputs["exact"]),
+            "relative_ladder": distance_over_every_ray(outputs["relative-ladder"],
+                                                       outputs["exact"]),
+        },
     }
-    result["pipeline"] = multisite_pipeline(session, stream, grids, batches[1], picks[1], out,
-                                            plain, batched)
     if rank == 0 and world == 1 and not args.skip_cpu:
-        result["error_vs_fp64_deg"] = multisite_accuracy(session, grids, regional, batches[1],
-                                                         picks[1], out, batched)
+        result["parity"] = multisite_parity(session, grids, regional, batch, outputs)
+    del outputs["exact"], outputs["ladder"]
+    result["pipeline"] = multisite_products(session, stream, grids, batch,
+                                            outputs["relative-ladder"], args)
     for dem in site_devs + [regional_dev]:
         dem.close()
     return result
 
 
-PIPELINE_CHUNK = 1024
-
-
-def multisite_pipeline(session, stream, grids, tiles, chosen, out, plain, batched):
-    """Horizons + one year of hourly sun-fraction bytes + PSR for one batch
-    of 16 site tiles.  Batched: the persistent ladder march, then the
-    lightmap as a CUDA graph of 1024-step chunks over all tiles, then PSR.
-    Plain: per tile, the per-tile march, the chunked lightmap and PSR
-    launched eagerly.  Both keep results in HBM; CUDA events."""
-    import ctypes
-
+def multisite_parity(session, grids, regional, batch, outputs):
+    """The 64-site batch against the oracle on MULTISITE_PARITY_RAYS random
+    rays spread over all tiles: the reference traversal against the FP32
+    oracle and the relative ladder against its FP32 restatement, bit for
+    bit; every traversal's distance from the FP64 restatement."""
     import torch
 
-    from lunarscout_b200 import _native, synthetic
-    from lunarscout_b200.contract import projection_array
-    from lunarscout_b200.graphs import DeviceGraph
-    from lunarscout_b200.lightmap_cuda import DeviceVectors
-
-    count = len(tiles)
-    plane = TILE * TILE
-    hours = synthetic.hours_between("2030-01-01T00", "2031-01-01T00", 1.0)
-    vectors = synthetic.sun_vectors(hours).astype(np.float32)
-    table = DeviceVectors(session.context, vectors)
-    steps = len(vectors)
-    patches = torch.zeros((count, TILE, TILE), dtype=torch.float32, device="cuda")
-    geo = np.zeros((count, 6), dtype=np.float64)
-    proj = np.zeros((count, 6), dtype=np.float64)
-    windows = np.zeros((count, 4), dtype=np.int32)
-    for i, (tile, site) in enumerate(zip(tiles, chosen)):
-        grid = grids[site]
-        vw = min(TILE, grid.width - tile.tile_column)
-        vh = min(TILE, grid.height - tile.tile_row)
-        patches[i, :vh, :vw] = torch.from_numpy(np.ascontiguousarray(
-            grid.elevation_m[tile.tile_row:tile.tile_row + vh,
-                             tile.tile_column:tile.tile_column + vw])).cuda()
-        geo[i] = grid.geo_transform
-        proj[i] = projection_array(grid.projection)
-        windows[i] = (tile.tile_column, tile.tile_row, vw, vh)
-    frames = torch.empty(count * plane * 12, dtype=torch.float32, device="cuda")
-    chunk_out = torch.empty((count, PIPELINE_CHUNK, plane), dtype=torch.uint8, device="cuda")
-    psr = torch.empty((count, plane), dtype=torch.uint8, device="cuda")
-    lib = _native.library()
-    blocks = [(start, min(PIPELINE_CHUNK, steps - start))
-              for start in range(0, steps, PIPELINE_CHUNK)]
-    torch.cuda.synchronize()
-
-    def lighting(first, n, signal, target):
-        _native.check(lib.ls200_lighting_device(
-            session.context, n, ctypes.c_void_p(patches[first].data_ptr()),
-            geo[first:].ctypes.data, proj[first:].ctypes.data, windows[first:].ctypes.data,
-            ctypes.c_void_p(out[first].data_ptr()), table.handle, 0, steps, signal,
-            ctypes.c_void_p(frames.data_ptr()), ctypes.c_void_p(target)))
-
-    def lightmap_chunks(first, n):
-        for start, length in blocks:
-            _native.check(lib.ls200_lighting_device(
-                session.context, n, ctypes.c_void_p(patches[first].data_ptr()),
-                geo[first:].ctypes.data, proj[first:].ctypes.data, windows[first:].ctypes.data,
-                ctypes.c_void_p(out[first].data_ptr()), table.handle, start, length, 1,
-                ctypes.c_void_p(frames.data_ptr()), ctypes.c_void_p(chunk_out.data_ptr())))
-
-    batched("ladder")(tiles)
-    torch.cuda.synchronize()
-    graph = DeviceGraph.capture(session.context, lambda: lightmap_chunks(0, count))
-
-    def timed(run):
-        run()
-        torch.cuda.synchronize()
-        start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        start.record(stream)
-        run()
-        end.record(stream)
-        torch.cuda.synchronize()
-        return start.elapsed_time(end) / 1000.0
-
-    def batched_pipeline():
-        batched("ladder")(tiles)
-        graph.launch()
-        lighting(0, count, 3, psr.data_ptr())
-
-    def plain_pipeline():
-        plain(tiles)
-        for i in range(count):
-            lightmap_chunks(i, 1)
-            lighting(i, 1, 3, psr[i].data_ptr())
-
-    try:
-        batched_s = timed(batched_pipeline)
-        plain_s = timed(plain_pipeline)
-        lightmap_graph_s = timed(graph.launch)
-        graph_nodes = graph.nodes
-    finally:
-        graph.close()
-        table.close()
-    rays = sum(w[2] * w[3] for w in windows) * AZIMUTHS
-    samples = sum(w[2] * w[3] for w in windows) * steps
-    return {
-        "tiles": count, "time_steps": steps, "chunk_steps": PIPELINE_CHUNK,
-        "graph_nodes_per_batch": graph_nodes,
-        "batched_seconds": batched_s, "plain_seconds": plain_s,
-        "speedup_batched_vs_plain": plain_s / batched_s,
-        "batched_rays_per_s": rays / batched_s,
-        "lightmap_graph_px_steps_per_s": samples / lightmap_graph_s,
-        "work": "ladder march (degrees) + sun-fraction bytes, 1 year hourly, in 1024-step "
-                "graph-captured chunks + PSR over the same vectors",
-    }
-
-
-def multisite_accuracy(session, grids, regional, tiles, chosen, out, batched):
-    """Horizon error of both traversals against the FP64 restatement of the
-    reference march on a bounded ray sample of the first timed batch."""
     import oracle
     from lunarscout_b200.contract import PyramidArrays, map_parameters, projection_parameters
 
@@ -648,39 +648,186 @@ def multisite_accuracy(session, grids, regional, tiles, chosen, out, batched):
                              projection_parameters(dem))
 
     regional_pyramid = pyramid(regional)
-    values = {}
-    for traversal in ("exact", "ladder"):
-        batched(traversal)(tiles)
-        values[traversal] = out[:4].cpu().numpy()
     rng = np.random.default_rng(9)
-    errors = {"exact": [], "ladder": []}
-    for i, (tile, site) in enumerate(list(zip(tiles, chosen))[:4]):
-        grid = grids[site]
+    per_tile = MULTISITE_PARITY_RAYS // len(batch) + 1
+    bits = {"exact": True, "relative-ladder": True}
+    errors = {name: [] for name in outputs}
+    rays = 0
+    for t, (tile, grid) in enumerate(zip(batch, grids)):
         width = min(TILE, grid.width - tile.tile_column)
         height = min(TILE, grid.height - tile.tile_row)
-        rows = rng.integers(0, height, ACCURACY_RAYS_PER_TILE)
-        cols = rng.integers(0, width, ACCURACY_RAYS_PER_TILE)
-        pixels = (rows * TILE + cols).astype(np.int32)
-        azimuths = rng.integers(0, AZIMUTHS, ACCURACY_RAYS_PER_TILE).astype(np.int32)
+        pixels = (rng.integers(0, height, per_tile) * TILE
+                  + rng.integers(0, width, per_tile)).astype(np.int32)
+        azimuths = rng.integers(0, AZIMUTHS, per_tile).astype(np.int32)
         segments = session.generate_segments(list(tile.dems), tile_column=tile.tile_column,
                                              tile_row=tile.tile_row, azimuth_count=AZIMUTHS,
                                              maximum_distance_m=RANGE_M,
                                              observer_elevation_m=OBSERVER_M)
-        fp64, _ = oracle.march_all_passes(segments, [pyramid(grid), regional_pyramid],
-                                          tile_column=tile.tile_column, tile_row=tile.tile_row,
-                                          observer_elevation_m=OBSERVER_M, pixels=pixels,
-                                          azimuths=azimuths, precision="f64")
-        reference = np.degrees(np.arctan(fp64))
-        for traversal in errors:
-            got = values[traversal][i][pixels, azimuths].astype(np.float64)
-            finite = np.isfinite(reference) & np.isfinite(got)
-            errors[traversal].append(np.abs(got[finite] - reference[finite]))
-    summary = {}
-    for traversal, parts in errors.items():
+        pyramids = [pyramid(grid), regional_pyramid]
+        common = dict(tile_column=tile.tile_column, tile_row=tile.tile_row,
+                      observer_elevation_m=OBSERVER_M, pixels=pixels, azimuths=azimuths)
+        index = (torch.from_numpy(pixels.astype(np.int64)).cuda(),
+                 torch.from_numpy(azimuths.astype(np.int64)).cuda())
+        got = {name: out[t][index].cpu().numpy() for name, out in outputs.items()}
+        expected = {
+            "exact": oracle.march_all_passes(segments, pyramids, **common)[0],
+            "relative-ladder": oracle.march_all_passes(
+                segments, pyramids, mask=oracle.ladder_mask(0, 1) | oracle.OPT_RELATIVE,
+                **common)[0],
+        }
+        for name, slopes in expected.items():
+            # The batch writes degrees with the device's slope -> degree
+            # conversion; apply the same conversion to the oracle's slopes.
+            degrees = session.slopes_to_degrees(slopes.reshape(1, -1)).reshape(-1)
+            bits[name] &= bool(np.array_equal(got[name], degrees))
+        fp64 = np.degrees(np.arctan(oracle.march_all_passes(segments, pyramids,
+                                                            precision="f64", **common)[0]))
+        finite = np.isfinite(fp64)
+        for name in outputs:
+            errors[name].append(np.abs(got[name][finite].astype(np.float64) - fp64[finite]))
+        rays += per_tile
+    summary = {"rays": rays, "tiles": len(batch),
+               "c3_bits_equal": bits["exact"],
+               "c3_relative_ladder_bits_equal": bits["relative-ladder"],
+               "error_vs_fp64_deg": {}}
+    for name, parts in errors.items():
         e = np.concatenate(parts)
-        summary[traversal] = {"p99.9": float(np.quantile(e, 0.999)), "max": float(e.max()),
-                              "mean": float(e.mean()), "rays": int(e.size)}
+        summary["error_vs_fp64_deg"][name] = {
+            "p99.9": float(np.quantile(e, 0.999)), "max": float(e.max()),
+            "over_0.01": int((e > 0.01).sum())}
     return summary
+
+
+def multisite_products(session, stream, grids, batch, horizons, args):
+    """The multi-site products over two years of hourly steps (17,545) on the
+    first C3_LIGHT_TILES tiles of the 64-site batch (all 64 with
+    --c3-full-lighting), from the relative-ladder horizons left in HBM by the
+    batched march: sun-fraction bytes, PSR against each site's reduced Sun
+    vectors (the reduction over that site's DEM, on the device), and the
+    Earth-visibility fraction.  The lightmap and PSR launches run eagerly and
+    then as one replayed CUDA graph (one node per launch over the whole
+    period); Earth visibility runs eagerly."""
+    import ctypes
+
+    import torch
+
+    from lunarscout_b200 import _native, synthetic
+    from lunarscout_b200.contract import projection_array
+    from lunarscout_b200.graphs import DeviceGraph
+    from lunarscout_b200.lightmap_cuda import DeviceVectors
+    from lunarscout_b200.psr_cuda import reduce_vectors_on
+
+    count = SITES if args.c3_full_lighting else C3_LIGHT_TILES
+    plane = TILE * TILE
+    hours = synthetic.hours_between("2030-01-01T00", "2032-01-01T00", 1.0)
+    steps = len(hours)
+    sun64, earth64 = synthetic.sun_vectors(hours), synthetic.earth_vectors(hours)
+    sun = DeviceVectors(session.context, sun64.astype(np.float32))
+    earth = DeviceVectors(session.context, earth64.astype(np.float32))
+    patches = torch.zeros((count, TILE, TILE), dtype=torch.float32, device="cuda")
+    geo = np.zeros((count, 6), dtype=np.float64)
+    proj = np.zeros((count, 6), dtype=np.float64)
+    windows = np.zeros((count, 4), dtype=np.int32)
+    started = time.perf_counter()
+    reduced = []
+    for i, tile in enumerate(batch[:count]):
+        grid = grids[i]
+        vw = min(TILE, grid.width - tile.tile_column)
+        vh = min(TILE, grid.height - tile.tile_row)
+        patches[i, :vh, :vw] = torch.from_numpy(np.ascontiguousarray(
+            grid.elevation_m[tile.tile_row:tile.tile_row + vh,
+                             tile.tile_column:tile.tile_column + vw])).cuda()
+        geo[i] = grid.geo_transform
+        proj[i] = projection_array(grid.projection)
+        windows[i] = (tile.tile_column, tile.tile_row, vw, vh)
+        vectors, _ = reduce_vectors_on(session.context, grid, sun64)
+        reduced.append(DeviceVectors(session.context, vectors.astype(np.float32)))
+    reduction_seconds = time.perf_counter() - started
+    # A ray with no terrain sample (-inf) is read as -50 deg, the value a
+    # stored tile decodes to there.
+    lit = horizons[:count]
+    lit.masked_fill_(torch.isneginf(lit), -50.0)
+    per_launch = 32
+    frames = torch.empty(min(count, per_launch) * plane * 12, dtype=torch.float32,
+                         device="cuda")
+    light = torch.empty((count, steps, plane), dtype=torch.uint8, device="cuda")
+    psr = torch.empty((count, plane), dtype=torch.uint8, device="cuda")
+    visible = torch.empty((count, plane), dtype=torch.float32, device="cuda")
+    lib = _native.library()
+    groups = [(first, min(per_launch, count - first)) for first in range(0, count, per_launch)]
+
+    def lighting(first, n, table, start, length, signal, target):
+        _native.check(lib.ls200_lighting_device(
+            session.context, n, ctypes.c_void_p(patches[first].data_ptr()),
+            geo[first:].ctypes.data, proj[first:].ctypes.data, windows[first:].ctypes.data,
+            ctypes.c_void_p(lit[first].data_ptr()), table.handle, start, length, signal,
+            ctypes.c_void_p(frames.data_ptr()), ctypes.c_void_p(target)))
+
+    def lightmap():
+        for first, n in groups:
+            lighting(first, n, sun, 0, steps, 1, light[first].data_ptr())
+
+    def psr_all():
+        for i in range(count):
+            lighting(i, 1, reduced[i], 0, reduced[i].count, 3, psr[i].data_ptr())
+
+    def visibility():
+        for first, n in groups:
+            _native.check(lib.ls200_earth_visibility_device(
+                session.context, n, ctypes.c_void_p(patches[first].data_ptr()),
+                geo[first:].ctypes.data, proj[first:].ctypes.data, windows[first:].ctypes.data,
+                ctypes.c_void_p(lit[first].data_ptr()), earth.handle, ctypes.c_float(0.0),
+                ctypes.c_void_p(visible[first].data_ptr())))
+
+    events = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+    torch.cuda.synchronize()
+    events[0].record(stream)
+    lightmap()
+    events[1].record(stream)
+    psr_all()
+    events[2].record(stream)
+    visibility()
+    events[3].record(stream)
+    torch.cuda.synchronize()
+    lightmap_s = events[0].elapsed_time(events[1]) / 1000.0
+    psr_s = events[1].elapsed_time(events[2]) / 1000.0
+    visibility_s = events[2].elapsed_time(events[3]) / 1000.0
+    graph = DeviceGraph.capture(session.context, lambda: (lightmap(), psr_all()))
+    try:
+        start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        start.record(stream)
+        graph.launch()
+        end.record(stream)
+        torch.cuda.synchronize()
+        graph_s = start.elapsed_time(end) / 1000.0
+        nodes = graph.nodes
+    finally:
+        graph.close()
+    pixels = int(sum(int(w[2]) * int(w[3]) for w in windows))
+    reduced_counts = [t.count for t in reduced]
+    psr_px_steps = sum(int(w[2]) * int(w[3]) * c for w, c in zip(windows, reduced_counts))
+    defined = torch.isfinite(visible)
+    result = {
+        "tiles": count, "of_batch_tiles": len(batch), "time_steps": steps,
+        "lightmap_px_steps_per_s": pixels * steps / lightmap_s,
+        "lightmap_seconds": lightmap_s,
+        "psr_reduced_vectors_mean": float(np.mean(reduced_counts)),
+        "psr_px_reduced_vectors_per_s": psr_px_steps / psr_s, "psr_seconds": psr_s,
+        "psr_fraction": float((psr == 255).float().mean()),
+        "vector_reduction_seconds_per_site": reduction_seconds / count,
+        "earth_visibility_px_steps_per_s": pixels * steps / visibility_s,
+        "earth_visibility_seconds": visibility_s,
+        "earth_visibility_mean": float(visible[defined].mean()),
+        "graph": {"nodes": nodes, "replay_seconds": graph_s,
+                  "eager_seconds": lightmap_s + psr_s,
+                  "replay_over_eager_throughput": (lightmap_s + psr_s) / graph_s,
+                  "work": "lightmap (whole period per launch) + PSR per tile"},
+        "work": "two years hourly: sun-fraction bytes, PSR over each site's reduced Sun "
+                "vectors, Earth-visibility fraction (margin >= 0)",
+    }
+    for table in reduced + [sun, earth]:
+        table.close()
+    return result
 
 
 GENERATE_SIDE = 512
@@ -815,11 +962,14 @@ SENSITIVITY_STEPS = 26281  # 3 years at 1 h
 def sensitivity_benchmark(session, regional, args, rank):
     """A slice of the large batched sensitivity run: an 8192 x 8192 primary
     at 5 m (the site recipe, 2400 craters) with the regional DEM, 8 tiles
-    around the centre, 200 km rays, 3 years of hourly Sun vectors.
-    Horizons by the persistent ladder march, PSR over all 26,281 vectors,
-    weights 1 within 500 m of each tile's PSR boundary, then the streamed
-    adjoint of the weighted mean smooth sun fraction in batches of 4 tiles
-    (the argmax checkpoints of one batch resident at a time)."""
+    around the centre, 200 km rays, 3 years of hourly Sun and Earth vectors.
+    Horizons by the persistent ladder march; PSR over the Sun vectors reduced
+    over the DEM (as the PSR product does) and over all of them; the Sun+Earth
+    mission-duration product (weekly candidate windows); weights 1 within
+    500 m of each tile's PSR boundary, then the streamed adjoint of the
+    weighted mean smooth sun fraction in batches of 4 tiles (the argmax
+    checkpoints of one batch resident at a time).  Peak device memory is the
+    high-water mark of the library's own allocations plus torch's."""
     import ctypes
 
     import torch
@@ -829,7 +979,11 @@ def sensitivity_benchmark(session, regional, args, rank):
     from lunarscout_b200.contract import projection_array
     from lunarscout_b200.cuda_backend import SiteTile
     from lunarscout_b200.lightmap_cuda import DeviceVectors
+    from lunarscout_b200.psr_cuda import reduce_vectors_on
 
+    torch.cuda.synchronize()
+    _native.memory_stats(session.device_id, reset_peak=True)
+    torch.cuda.reset_peak_memory_stats()
     started = time.perf_counter()
     primary = synthetic.site_dem(SENSITIVITY_SIDE, 5.0, craters=2400, seed=5)
     build_s = time.perf_counter() - started
@@ -837,7 +991,9 @@ def sensitivity_benchmark(session, regional, args, rank):
     tiles = [(centre + dx * TILE, centre + dy * TILE) for dy in (-1, 0) for dx in (-2, -1, 0, 1)]
     count = len(tiles)
     plane = TILE * TILE
-    vectors = synthetic.sun_vectors(np.arange(SENSITIVITY_STEPS, dtype=np.float64))
+    hours = np.arange(SENSITIVITY_STEPS, dtype=np.float64)
+    vectors = synthetic.sun_vectors(hours)
+    earth_vectors = synthetic.earth_vectors(hours)
     dems = [session.upload_dem_grid(primary), session.upload_dem_grid(regional)]
     horizons = torch.empty((count, plane, AZIMUTHS), dtype=torch.float32, device="cuda")
     site_tiles = [SiteTile(tuple(dems), tx, ty, RANGE_M, OBSERVER_M) for tx, ty in tiles]
@@ -851,28 +1007,59 @@ def sensitivity_benchmark(session, regional, args, rank):
     proj = np.ascontiguousarray(np.repeat(projection_array(primary.projection)[None, :],
                                           count, 0))
     windows = np.array([(tx, ty, TILE, TILE) for tx, ty in tiles], dtype=np.int32)
+    started = time.perf_counter()
+    reduced_vectors, reduced_indices = reduce_vectors_on(session.context, primary, vectors)
+    reduction_s = time.perf_counter() - started
     table = DeviceVectors(session.context, vectors.astype(np.float32))
+    reduced_table = DeviceVectors(session.context, reduced_vectors.astype(np.float32))
+    earth = DeviceVectors(session.context, earth_vectors.astype(np.float32))
     frames = torch.empty(count * plane * 12, dtype=torch.float32, device="cuda")
     psr = torch.empty((count, plane), dtype=torch.uint8, device="cuda")
+    psr_all = torch.empty((count, plane), dtype=torch.uint8, device="cuda")
     lib = _native.library()
 
-    def psr_launch():
+    def psr_launch(vector_table, target):
         _native.check(lib.ls200_lighting_device(
             session.context, count, ctypes.c_void_p(patches.data_ptr()), geo.ctypes.data,
             proj.ctypes.data, windows.ctypes.data, ctypes.c_void_p(horizons.data_ptr()),
-            table.handle, 0, SENSITIVITY_STEPS, 3, ctypes.c_void_p(frames.data_ptr()),
-            ctypes.c_void_p(psr.data_ptr())))
+            vector_table.handle, 0, vector_table.count, 3, ctypes.c_void_p(frames.data_ptr()),
+            ctypes.c_void_p(target.data_ptr())))
 
-    psr_launch()
-    torch.cuda.synchronize()
-    begin, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    begin.record()
-    psr_launch()
-    end.record()
-    torch.cuda.synchronize()
-    psr_s = begin.elapsed_time(end) / 1000.0
-    table.close()
+    def timed(run):
+        run()
+        torch.cuda.synchronize()
+        begin, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        begin.record()
+        run()
+        end.record()
+        torch.cuda.synchronize()
+        return begin.elapsed_time(end) / 1000.0
+
+    psr_s = timed(lambda: psr_launch(reduced_table, psr))
+    psr_all_s = timed(lambda: psr_launch(table, psr_all))
+    # Sun + Earth mission duration: condition = fraction >= 0.5 and Earth
+    # margin >= 0, weekly candidate start windows, 1 h samples.
+    week = 7 * 24
+    starts = np.arange(0, SENSITIVITY_STEPS - week, week, dtype=np.int32)
+    start_windows = np.ascontiguousarray(np.stack([starts, starts + week], axis=1))
+    sample_hours = np.ones(SENSITIVITY_STEPS, dtype=np.float64)
+    mission = torch.empty((count, len(starts), plane), dtype=torch.float32, device="cuda")
+
+    def mission_launch():
+        _native.check(lib.ls200_mission_duration_device(
+            session.context, count, ctypes.c_void_p(patches.data_ptr()), geo.ctypes.data,
+            proj.ctypes.data, windows.ctypes.data, ctypes.c_void_p(horizons.data_ptr()),
+            table.handle, earth.handle, ctypes.c_float(0.5), ctypes.c_float(0.0),
+            sample_hours.ctypes.data, start_windows.ctypes.data, len(starts), 0,
+            ctypes.c_void_p(mission.data_ptr())))
+
+    mission_s = timed(mission_launch)
+    for t in (table, reduced_table, earth):
+        t.close()
     masks = psr.cpu().numpy().reshape(count, TILE, TILE)
+    band = None
+    if rank == 0 and not args.skip_cpu:
+        band = psr_band(primary, horizons[0], reduced_vectors, masks[0], tiles[0])
     weights = np.stack([psr_boundary_weights(m, 5.0, 500.0) for m in masks])
     del horizons
     for dem in dems:
@@ -886,28 +1073,63 @@ def sensitivity_benchmark(session, regional, args, rank):
     try:
         loss, grads = streamed.value_and_gradient(heights)
         seconds = dict(streamed.last_seconds)
-        free, total = torch.cuda.mem_get_info()
         nonzero = int(torch.count_nonzero(grads[0]))
     finally:
         streamed.close()
+    torch.cuda.synchronize()
+    _, library_peak = _native.memory_stats(session.device_id)
+    torch_peak = torch.cuda.max_memory_allocated()
     forward_s = seconds["forward_march"] + seconds["forward_lighting"]
     rays = count * plane * AZIMUTHS
     return {
         "workload": "8 tiles of an 8192x8192 5 m primary + 240 m regional, 200 km rays, "
-                    "3 years hourly (26,281 Sun vectors)",
+                    f"3 years hourly ({SENSITIVITY_STEPS:,} Sun and Earth vectors)",
         "tiles": count, "batch_tiles": SENSITIVITY_BATCH, "time_steps": SENSITIVITY_STEPS,
         "dem_build_s": build_s,
         "march_rays_per_s": rays / march_s,
-        "psr_px_steps_per_s": count * plane * SENSITIVITY_STEPS / psr_s,
+        "psr_reduced_vectors": int(len(reduced_indices)),
+        "psr_vector_reduction_s": reduction_s,
+        "psr_px_reduced_vectors_per_s": count * plane * len(reduced_indices) / psr_s,
+        "psr_ms_per_tile": 1000.0 * psr_s / count,
+        "psr_all_vectors_px_steps_per_s": count * plane * SENSITIVITY_STEPS / psr_all_s,
         "psr_fraction": float((masks > 0).mean()),
+        "psr_fraction_all_vectors": float((psr_all.cpu().numpy() > 0).mean()),
+        "psr_band": band,
+        "mission_sun_earth": {"windows": int(len(starts)), "window_hours": week,
+                              "px_steps_per_s": count * plane * SENSITIVITY_STEPS / mission_s,
+                              "seconds": mission_s,
+                              "mean_longest_hours": float(mission.mean())},
         "weighted_fraction": float(weights.mean()),
         "loss": loss, "forward_s": forward_s, "backward_s": seconds["backward"],
         "adjoint_over_forward": seconds["backward"] / forward_s,
         "gradient_nonzero_cells": nonzero,
-        "device_memory_in_use_gb": (total - free) / 1e9,
-        "memory_note": "cudaMemGetInfo after the run; the library keeps its largest buffers, "
-                       "so this includes the run's peak",
+        "peak_device_memory_gb": {
+            "library_high_water": library_peak / 1e9,
+            "torch_high_water": torch_peak / 1e9,
+            "bound": (library_peak + torch_peak) / 1e9,
+            "note": "high-water marks of the library's own allocations "
+                    "(ls200_memory_stats) and of torch's caching allocator over this leg; "
+                    "their sum bounds the leg's peak"},
     }
+
+
+def psr_band(primary, horizons, vectors, mask, tile):
+    """The device PSR mask of one tile against the oracle's (the reference's
+    FP64 PSR on the same reduced vectors): pixels that differ, the pixels of
+    the 1e-4 deg band around the limb threshold, and differences outside it."""
+    from oracle import products
+
+    tx, ty = tile
+    host = horizons.cpu().numpy().reshape(TILE, TILE, AZIMUTHS)
+    host = np.where(np.isneginf(host), np.float32(-50.0), host)
+    started = time.perf_counter()
+    expected = products.psr_tile(primary, host, vectors, tile_y=ty, tile_x=tx)
+    peak = products.psr_peak_margin(primary, host, vectors, tile_y=ty, tile_x=tx)
+    in_band = np.abs(peak - products.PSR_LIMB_THRESHOLD) < 1e-4
+    differ = mask != expected
+    return {"pixels": int(mask.size), "band_pixels": int(in_band.sum()),
+            "differ": int(differ.sum()), "differ_outside_band": int((differ & ~in_band).sum()),
+            "oracle_seconds": time.perf_counter() - started}
 
 
 def run_ours(args):
@@ -993,40 +1215,50 @@ def run_ours(args):
     rays = world * args.steps * RAYS_PER_TILE
     value = rays / elapsed
 
-    # End to end through the drop-in session call with pinned host buffers.
-    e2e_value = None
+    # End to end through the drop-in session call with pinned host buffers,
+    # over the same timed tiles as `value`: each call copies its tile's
+    # segments host -> device and reads the slopes back into host memory.
     h2d = int(np.prod(segment_shape)) * 4
     d2h = TILE * TILE * AZIMUTHS * 4
-    from lunarscout_b200.contract import PyramidArrays
-
-    class _Pyr:  # the session's resident-pyramid cache keys on identity
-        pass
-
     e2e_session = CudaSession(local)
-    host_pyramids = []
-    for dem in (primary, regional):
-        p = e2e_session.build_max_pyramid(dem)
-        host_pyramids.append(p)
-    host_segments = [pinned_empty(segment_shape, np.float32) for _ in range(2)]
-    for i in range(2):
-        host_segments[i][...] = segments[args.warmup + i].cpu().numpy()
-    e2e_session.subpatch_hierarchical_all_passes(host_segments[0], host_pyramids,
-                                                 tile_column=tiles[args.warmup][1],
-                                                 tile_row=tiles[args.warmup][0],
-                                                 tile_width=TILE, tile_height=TILE,
-                                                 subpatch_size=8)
-    e2e_steps = max(2, min(args.steps, 6))
+    host_pyramids = [e2e_session.build_max_pyramid(dem) for dem in (primary, regional)]
+    host_segments = []
+    for k in range(args.warmup, total_steps):
+        buffer = pinned_empty(segment_shape, np.float32)
+        buffer[...] = segments[k].cpu().numpy()
+        host_segments.append(buffer)
+
+    def e2e_call(k):
+        tile_row, tile_column = tiles[k]
+        slopes, _ = e2e_session.subpatch_hierarchical_all_passes(
+            host_segments[k - args.warmup], host_pyramids, tile_column=tile_column,
+            tile_row=tile_row, tile_width=TILE, tile_height=TILE, subpatch_size=8)
+        return slopes
+
+    e2e_call(args.warmup)
     if world > 1:
         dist.barrier()
     started = time.perf_counter()
-    for k in range(e2e_steps):
-        index = args.warmup + (k % 2)
-        e2e_session.subpatch_hierarchical_all_passes(
-            host_segments[k % 2], host_pyramids, tile_column=tiles[index][1],
-            tile_row=tiles[index][0], tile_width=TILE, tile_height=TILE, subpatch_size=8)
+    for k in range(args.warmup, total_steps):
+        e2e_call(k)
     e2e_elapsed = max_over_ranks(time.perf_counter() - started, world)
-    e2e_value = world * e2e_steps * RAYS_PER_TILE / e2e_elapsed
+    e2e_value = world * args.steps * RAYS_PER_TILE / e2e_elapsed
     e2e_session.close()
+    del host_segments
+
+    parity = None
+    if rank == 0 and world == 1 and not args.skip_cpu:
+        parity = site_parity(session, dems, primary, regional, segments[args.warmup],
+                             tiles[args.warmup])
+    numba_reference = None
+    if rank == 0 and world == 1 and not args.skip_reference_numba:
+        tile_row, tile_column = tiles[args.warmup]
+        step(args.warmup)
+        torch.cuda.synchronize()
+        numba_reference = reference_numba_cuda(primary, regional, segments[args.warmup],
+                                               tiles[args.warmup], output.cpu().numpy())
+        numba_reference["ours_rays_per_s_device"] = value
+        numba_reference["ours_rays_per_s_e2e"] = e2e_value
 
     lighting = lighting_benchmark(session, dems, segments, tiles, primary, args, world, rank)
     del segments
@@ -1084,6 +1316,8 @@ def run_ours(args):
             "gpu_launches": 3 * args.steps,
             "clocks": clocks,
             "segment_generation_ms_per_tile": segment_seconds * 1000.0,
+            "parity": parity,
+            "reference_numba_cuda": numba_reference,
             "lightmap": lighting,
             "multisite": multisite,
             "adjoint": adjoint,
@@ -1094,6 +1328,135 @@ def run_ours(args):
     session.close()
     if world > 1:
         dist.destroy_process_group()
+
+
+PARITY_RAYS = 20_000
+
+
+def site_parity(session, dems, primary, regional, device_segments, tile):
+    """Bit parity of the timed march with the FP32 oracle on PARITY_RAYS
+    random rays of the first timed site-scale tile (1440 azimuths, 200 km,
+    both passes), and the distance of the reference and relative FP32
+    arithmetic from the FP64 restatement on the same rays."""
+    import torch
+
+    import oracle
+    from lunarscout_b200.contract import PyramidArrays, map_parameters, projection_parameters
+    from lunarscout_b200.cuda_backend import SiteTile
+
+    tile_row, tile_column = tile
+    out = torch.empty((TILE * TILE, AZIMUTHS), dtype=torch.float32, device="cuda")
+    torch.cuda.synchronize()
+    # The timed call, into a fresh buffer.
+    session.march_all_passes_device(device_segments.data_ptr(), AZIMUTHS, (TILE // 8 + 2) ** 2,
+                                    dems, tile_column=tile_column, tile_row=tile_row,
+                                    observer_elevation_m=OBSERVER_M, device_out=out.data_ptr())
+    session.synchronize()
+    timed = out.cpu().numpy()
+    session.march_sites([SiteTile(tuple(dems), tile_column, tile_row, RANGE_M, OBSERVER_M)],
+                        device_out=out.data_ptr(), azimuth_count=AZIMUTHS,
+                        traversal="relative")
+    torch.cuda.synchronize()
+    relative = out.cpu().numpy()
+    segments = device_segments.cpu().numpy()
+    pyramids = []
+    for dem in (primary, regional):
+        mips, levels = oracle.build_pyramid(dem.elevation_m)
+        pyramids.append(PyramidArrays(dem.elevation_m, mips, levels, map_parameters(dem),
+                                      projection_parameters(dem)))
+    rng = np.random.default_rng(2024)
+    pixels = rng.integers(0, TILE * TILE, PARITY_RAYS).astype(np.int32)
+    azimuths = rng.integers(0, AZIMUTHS, PARITY_RAYS).astype(np.int32)
+    common = dict(tile_column=tile_column, tile_row=tile_row, observer_elevation_m=OBSERVER_M,
+                  pixels=pixels, azimuths=azimuths)
+    fp32, _ = oracle.march_all_passes(segments, pyramids, **common)
+    fp32_relative, _ = oracle.march_all_passes(
+        segments, pyramids, mask=oracle.PRODUCTION_MASK | oracle.OPT_RELATIVE, **common)
+    fp64, _ = oracle.march_all_passes(segments, pyramids, precision="f64", **common)
+    got = timed[pixels, azimuths]
+    got_relative = relative[pixels, azimuths]
+    reference = np.degrees(np.arctan(fp64))
+
+    def distance(values):
+        d = np.abs(np.degrees(np.arctan(values.astype(np.float64))) - reference)
+        d = d[np.isfinite(reference)]
+        return {"p99.9": float(np.quantile(d, 0.999)), "max": float(d.max()),
+                "over_0.01": int((d > 0.01).sum())}
+
+    return {
+        "workload": "first timed site-scale tile, 1440 az, 200 km, both passes",
+        "rays": PARITY_RAYS,
+        "c2_bits_equal": bool(np.array_equal(got, fp32)),
+        "c2_relative_bits_equal": bool(np.array_equal(got_relative, fp32_relative)),
+        "error_vs_fp64_deg": {"reference_arithmetic": distance(got),
+                              "relative_arithmetic": distance(got_relative)},
+    }
+
+
+def reference_runtime():
+    """The reference installed under baseline/_ref (None when absent)."""
+    sys.path.insert(0, str(ROOT / "baseline"))
+    import load_reference
+
+    return load_reference if load_reference.available() else None
+
+
+def reference_dem(ours):
+    """This project's DemGrid as the reference's own DemGrid."""
+    from lunarscout._numba_horizon import geometry
+
+    return geometry.DemGrid(np.ascontiguousarray(ours.elevation_m, dtype=np.float32),
+                            np.array(ours.geo_transform, dtype=np.float64),
+                            geometry.ProjectionParameters.from_array(ours.projection.as_array()))
+
+
+def reference_numba_cuda(primary, regional, device_segments, tile, ours_slopes, repeats=2):
+    """The reference's own Numba-CUDA march (cuda_backend.CudaSession.
+    subpatch_hierarchical_all_passes, cuda_backend.py:1445-1552) on the same
+    B200, the same site-scale tile and the same segments as the timed march:
+    its rays/s through that drop-in call (host segments in, host slopes out)
+    and from its own per-pass CUDA-event times, and its slopes against ours."""
+    runtime = reference_runtime()
+    if runtime is None:
+        return {"available": False, "reason": "reference not installed under baseline/_ref"}
+    try:
+        runtime.import_reference(enable_numba_cuda=True)
+        from lunarscout._numba_horizon import cuda_backend
+
+        session = cuda_backend.CudaSession(device_id=0)
+        pyramids = [session.build_max_pyramid(reference_dem(d)) for d in (primary, regional)]
+        values = device_segments.cpu().numpy()
+        tile_row, tile_column = tile
+        kwargs = dict(tile_column=tile_column, tile_row=tile_row, tile_width=TILE,
+                      tile_height=TILE, subpatch_size=8, observer_elevation_m=OBSERVER_M)
+        started = time.perf_counter()
+        slopes, _ = session.subpatch_hierarchical_all_passes(values, pyramids, **kwargs)
+        first_call_s = time.perf_counter() - started
+        walls, kernels = [], []
+        for _ in range(repeats):
+            started = time.perf_counter()
+            slopes, pass_seconds = session.subpatch_hierarchical_all_passes(values, pyramids,
+                                                                             **kwargs)
+            walls.append(time.perf_counter() - started)
+            kernels.append(float(sum(pass_seconds)))
+    except Exception as error:  # the JIT or the device refused: record why
+        return {"available": False, "reason": f"{type(error).__name__}: {error}"[:400]}
+    theirs = np.degrees(np.arctan(np.asarray(slopes, dtype=np.float64)))
+    ours = np.degrees(np.arctan(np.asarray(ours_slopes, dtype=np.float64)))
+    finite = np.isfinite(theirs) & np.isfinite(ours)
+    wall, kernel = min(walls), min(kernels)
+    return {
+        "available": True,
+        "how": "numba's built-in CUDA target in place of the numba-cuda package "
+               "(lunarscout/_cuda_runtime.py:12 gate replaced), unmodified kernels",
+        "rays_per_s_call": RAYS_PER_TILE / wall,
+        "rays_per_s_kernel_events": RAYS_PER_TILE / kernel,
+        "call_seconds": wall, "kernel_seconds": kernel,
+        "first_call_seconds_with_jit": first_call_s,
+        "slopes_bits_equal_fraction": float(np.mean(np.asarray(slopes) == ours_slopes)),
+        "max_abs_deg_vs_ours": float(np.abs(theirs - ours)[finite].max()),
+        "same_inf_rays": bool(np.array_equal(np.isinf(theirs), np.isinf(ours))),
+    }
 
 
 def run_profile_case():
@@ -1198,6 +1561,11 @@ def main():
                         help="leave out the end-to-end tile-generator leg")
     parser.add_argument("--skip-sensitivity", action="store_true",
                         help="leave out the 8192^2 streamed-adjoint sensitivity slice")
+    parser.add_argument("--skip-reference-numba", action="store_true",
+                        help="leave out the reference's own Numba-CUDA march on the same tile")
+    parser.add_argument("--c3-full-lighting", action="store_true",
+                        help="run the multi-site products over all 64 tiles of the batch "
+                             f"(default: the first {C3_LIGHT_TILES})")
     parser.add_argument("--profile", nargs="?", const="site", choices=("site", "multisite"),
                         help="small profiling case, no timing: 'site' = one site-scale tile "
                              "(two march steps, two lighting launches); 'multisite' = four "

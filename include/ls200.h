@@ -224,6 +224,19 @@ ls200_status ls200_lighting_run(ls200_context *ctx, const ls200_vectors *vectors
 /* PSR byte mask (255 = permanently shadowed) of the staged patch over all
  * vectors into host out[128*128]. */
 ls200_status ls200_psr_run(ls200_context *ctx, const ls200_vectors *vectors, uint8_t *out);
+/* The PSR vector reduction, replacing reduce_sun_vectors_for_psr
+ * (src/lunarscout/_numba_horizon/psr.py:61-91, called once per product at
+ * psr_pipeline.py:259-263): for the DEM's four corner pixels and its centre
+ * pixel and 1440 azimuth bins of 0.25 deg, the index of the highest vector
+ * (first on ties), listed viewpoint by viewpoint, bin by bin, each index once
+ * in order of first appearance.  FP64 on the device.  dem: host float32
+ * [height, width] (only the five viewpoints' elevations are read);
+ * vectors: host float64 [count, 3] Moon-ME metres; indices_out: room for
+ * 7200 int64; *reduced_count receives how many were written.  Synchronous. */
+ls200_status ls200_psr_reduce_vectors(ls200_context *ctx, const float *dem, int width,
+                                      int height, const double *geo_transform,
+                                      const double *projection, const double *vectors,
+                                      int count, int64_t *indices_out, int *reduced_count);
 /* Device-resident batch of up to 32 patches: device patch_dems
  * [n,128,128], host geo_transforms/projections [n,6] f64, host windows
  * [n,4] (tile_x, tile_y, valid_width, valid_height), device horizons
@@ -380,6 +393,13 @@ ls200_status ls200_sun_loss_checkpoints(ls200_context *ctx, float *points, uint8
  * measured denominator of the march's FP32 roofline.  No reference
  * counterpart. */
 ls200_status ls200_fp32_probe(ls200_context *ctx, int iterations, double *tflops);
+
+/* Device memory held by this library's own allocations on `device` (DEMs,
+ * vector tables, context buffers; not the caller's buffers): bytes in use now
+ * and the high-water mark since load or the last reset; reset_peak != 0 sets
+ * the mark to the bytes in use.  Either pointer may be NULL.  No reference
+ * counterpart (the reference reports cudaMemGetInfo snapshots). */
+ls200_status ls200_memory_stats(int device, int64_t *in_use, int64_t *peak, int reset_peak);
 
 #ifdef __cplusplus
 }

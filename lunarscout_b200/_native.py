@@ -113,6 +113,8 @@ SIGNATURES: dict[str, list] = {
     "ls200_lighting_load": [_vp, _f32p, _f64p, _f64p, _f32p, _i, _i, _i, _i],
     "ls200_lighting_run": [_vp, _vp, _i, _i, _i, _vp],
     "ls200_psr_run": [_vp, _vp, _vp],
+    "ls200_psr_reduce_vectors": [_vp, _f32p, _i, _i, _f64p, _f64p, _f64p, _i, _vp, _vp],
+    "ls200_memory_stats": [_i, _vp, _vp, _i],
     "ls200_lighting_device": [_vp, _i, _vp, _vp, _vp, _vp, _vp, _vp, _i, _i, _i, _vp, _vp],
     "ls200_sun_fraction": [_vp, _f32p, _f32p, _f32p, _i, _f32p],
     "ls200_lighting_device_noalloc": [_vp, _i, _vp, _vp, _vp, _vp, _vp, _vp, _i, _i, _i, _i,
@@ -244,3 +246,12 @@ def _free_host(address: int) -> None:
         library().ls200_host_free(ctypes.c_void_p(address))
     except Exception:  # pragma: no cover - interpreter shutdown
         pass
+
+
+def memory_stats(device: int = 0, *, reset_peak: bool = False) -> tuple[int, int]:
+    """(bytes in use, high-water mark) of this library's own device
+    allocations on `device` (ls200_memory_stats)."""
+    in_use, peak = ctypes.c_int64(0), ctypes.c_int64(0)
+    call("ls200_memory_stats", int(device), ctypes.byref(in_use), ctypes.byref(peak),
+         1 if reset_peak else 0)
+    return int(in_use.value), int(peak.value)

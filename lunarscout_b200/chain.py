@@ -226,11 +226,29 @@ class ProductChain:
             table.close()
         return out
 
-    def psr(self, batch: PatchBatch, sun_vectors_m) -> list:
-        """uint8 PSR masks [valid_h, valid_w] per patch (psr_cuda.py:57-186),
-        for the (already reduced) vectors given, as PsrCudaSession.compute_patch."""
+    def reduced_sun_vectors(self, sun_vectors_m) -> tuple[np.ndarray, np.ndarray]:
+        """The PSR product's vector reduction over the primary DEM
+        (reduce_sun_vectors_for_psr, psr.py:61-91, on the device), cached
+        for the last vector table."""
+        from .psr_cuda import reduce_vectors_on
+
+        vectors = np.ascontiguousarray(sun_vectors_m, dtype=np.float64)
+        key = (vectors.shape, vectors.tobytes())
+        if getattr(self, "_reduction_key", None) != key:
+            self._reduction = reduce_vectors_on(self.session.context, self.primary, vectors)
+            self._reduction_key = key
+        return self._reduction
+
+    def psr(self, batch: PatchBatch, sun_vectors_m, *, reduce: bool = True) -> list:
+        """uint8 PSR masks [valid_h, valid_w] per patch: the PSR product of
+        psr_pipeline.py:259-263 — the vectors reduced over the primary DEM
+        (reduced_sun_vectors), then psr_cuda.py:57-186 on each patch.  With
+        ``reduce=False`` the vectors given are used as they are, as
+        PsrCudaSession.compute_patch does."""
         import torch
 
+        if reduce:
+            sun_vectors_m = self.reduced_sun_vectors(sun_vectors_m)[0]
         vectors = np.ascontiguousarray(validate_vectors(sun_vectors_m), dtype=np.float32)
         out = torch.empty((len(batch), PIXEL_COUNT), dtype=torch.uint8, device="cuda")
         frames = torch.empty(len(batch) * PIXEL_COUNT * 12, dtype=torch.float32, device="cuda")

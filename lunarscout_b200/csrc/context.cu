@@ -90,9 +90,9 @@ ls200_status ls200_context_destroy(ls200_context *ctx) {
         cudaStreamSynchronize(ctx->stream);
         // DEMs still alive belong to this context: release them with it.
         for (ls200_dem *dem : ctx->dems) {
-            if (dem->level0) cudaFree(dem->level0);
-            if (dem->cells) cudaFree(dem->cells);
-            if (dem->bounds) cudaFree(dem->bounds);
+            if (dem->level0) tracked_free(dem->level0);
+            if (dem->cells) tracked_free(dem->cells);
+            if (dem->bounds) tracked_free(dem->bounds);
             delete dem;
         }
         ctx->dems.clear();
@@ -191,10 +191,10 @@ ls200_status ls200_dem_create(ls200_context *ctx, const float *level0, int width
             const size_t cells0 = size_t(width) * height;
             LS_REQUIRE(cells0 + size_t(dem->mip_count) < (size_t(1) << 31),
                        "DEM pyramid exceeds the int32 cell index range");
-            LS_CUDA(cudaMalloc(&dem->level0, sizeof(float) * cells0));
+            LS_CUDA(tracked_malloc(&dem->level0, sizeof(float) * cells0));
             // One allocation: sanitized level 0 followed by the packed mips.
-            LS_CUDA(cudaMalloc(&dem->cells, sizeof(float) * (cells0 + size_t(dem->mip_count))));
-            LS_CUDA(cudaMalloc(&dem->bounds, sizeof(float) * (cells0 + size_t(dem->mip_count))));
+            LS_CUDA(tracked_malloc(&dem->cells, sizeof(float) * (cells0 + size_t(dem->mip_count))));
+            LS_CUDA(tracked_malloc(&dem->bounds, sizeof(float) * (cells0 + size_t(dem->mip_count))));
             dem->mips = dem->cells + cells0;
             LS_CUDA(cudaMemcpyAsync(dem->level0, level0, sizeof(float) * cells0,
                                     cudaMemcpyHostToDevice, ctx->stream));
@@ -209,9 +209,9 @@ ls200_status ls200_dem_create(ls200_context *ctx, const float *level0, int width
             LS_CUDA(cudaStreamSynchronize(ctx->stream));
             ctx->dems.insert(dem);
         } catch (...) {
-            if (dem->level0) cudaFree(dem->level0);
-            if (dem->cells) cudaFree(dem->cells);
-            if (dem->bounds) cudaFree(dem->bounds);
+            if (dem->level0) tracked_free(dem->level0);
+            if (dem->cells) tracked_free(dem->cells);
+            if (dem->bounds) tracked_free(dem->bounds);
             delete dem;
             throw;
         }
@@ -226,9 +226,9 @@ ls200_status ls200_dem_destroy(ls200_dem *dem) {
         activate(dem->ctx);
         cudaStreamSynchronize(dem->ctx->stream);
         dem->ctx->dems.erase(dem);
-        if (dem->level0) cudaFree(dem->level0);
-        if (dem->cells) cudaFree(dem->cells);
-        if (dem->bounds) cudaFree(dem->bounds);
+        if (dem->level0) tracked_free(dem->level0);
+        if (dem->cells) tracked_free(dem->cells);
+        if (dem->bounds) tracked_free(dem->bounds);
         delete dem;
     });
 }

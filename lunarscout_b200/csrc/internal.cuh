@@ -66,22 +66,32 @@ ls200_status guard(F &&body) {
     }
 }
 
+// Device allocations of the library go through these two calls, which keep a
+// per-device count of the bytes in use and its high-water mark
+// (ls200_memory_stats).
+cudaError_t tracked_malloc_bytes(void **ptr, size_t bytes);
+cudaError_t tracked_free(void *ptr);
+template <class T>
+cudaError_t tracked_malloc(T **ptr, size_t bytes) {
+    return tracked_malloc_bytes(reinterpret_cast<void **>(ptr), bytes);
+}
+
 // A growable device buffer owned by a context.
 struct DeviceBuffer {
     void *ptr = nullptr;
     size_t bytes = 0;
     void reserve(size_t n) {
         if (n <= bytes) return;
-        if (ptr) cudaFree(ptr);
+        if (ptr) tracked_free(ptr);
         ptr = nullptr;
         bytes = 0;
-        LS_CUDA(cudaMalloc(&ptr, n));
+        LS_CUDA(tracked_malloc(&ptr, n));
         bytes = n;
     }
     template <class T>
     T *as() const { return static_cast<T *>(ptr); }
     ~DeviceBuffer() {
-        if (ptr) cudaFree(ptr);
+        if (ptr) tracked_free(ptr);
     }
 };
 

@@ -26,9 +26,9 @@ static LightingState &state_of(ls200_context *ctx) {
 void release_lighting_state(ls200_context *ctx) {
     if (!ctx->lighting) return;
     for (ls200_vectors *v : ctx->lighting->vectors) {
-        cudaFree(v->data);
-        cudaFree(v->order);
-        cudaFree(v->window);
+        tracked_free(v->data);
+        tracked_free(v->order);
+        tracked_free(v->window);
         delete v;
     }
     delete ctx->lighting;
@@ -79,14 +79,14 @@ ls200_status ls200_vectors_create(ls200_context *ctx, const float *vectors, int 
         v->ctx = ctx;
         v->count = count;
         auto release = [&] {
-            if (v->data) cudaFree(v->data);
-            if (v->order) cudaFree(v->order);
-            if (v->window) cudaFree(v->window);
+            if (v->data) tracked_free(v->data);
+            if (v->order) tracked_free(v->order);
+            if (v->window) tracked_free(v->window);
             delete v;
         };
-        cudaError_t e = cudaMalloc(&v->data, sizeof(float) * 3 * size_t(count));
-        if (e == cudaSuccess) e = cudaMalloc(&v->order, sizeof(int) * size_t(count));
-        if (e == cudaSuccess) e = cudaMalloc(&v->window, sizeof(int) * size_t(count));
+        cudaError_t e = tracked_malloc(&v->data, sizeof(float) * 3 * size_t(count));
+        if (e == cudaSuccess) e = tracked_malloc(&v->order, sizeof(int) * size_t(count));
+        if (e == cudaSuccess) e = tracked_malloc(&v->window, sizeof(int) * size_t(count));
         if (e != cudaSuccess) {
             release();
             throw Error(LS200_ERR_CUDA, std::string("cudaMalloc: ") + cudaGetErrorString(e));
@@ -113,9 +113,9 @@ ls200_status ls200_vectors_destroy(ls200_vectors *vectors) {
         activate(vectors->ctx);
         cudaStreamSynchronize(vectors->ctx->stream);
         state_of(vectors->ctx).vectors.erase(vectors);
-        cudaFree(vectors->data);
-        cudaFree(vectors->order);
-        cudaFree(vectors->window);
+        tracked_free(vectors->data);
+        tracked_free(vectors->order);
+        tracked_free(vectors->window);
         delete vectors;
     });
 }

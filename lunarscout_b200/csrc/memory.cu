@@ -1,7 +1,44 @@
-// Pinned host buffers and the FP32-issue reference probe of the ls200 C ABI.
+// Pinned host buffers, device-allocation accounting and the FP32-issue
+// reference probe of the ls200 C ABI.
+#include <unordered_map>
+
 #include "internal.cuh"
 
 namespace ls200 {
+
+namespace {
+constexpr int kTrackedDevices = 64;
+std::mutex g_memory_lock;
+std::unordered_map<void *, std::pair<int, size_t>> g_allocations;
+int64_t g_in_use[kTrackedDevices] = {};
+int64_t g_peak[kTrackedDevices] = {};
+}  // namespace
+
+cudaError_t tracked_malloc_bytes(void **ptr, size_t bytes) {
+    const cudaError_t e = cudaMalloc(ptr, bytes);
+    if (e != cudaSuccess) return e;
+    int device = 0;
+    cudaGetDevice(&device);
+    if (device < 0 || device >= kTrackedDevices) device = 0;
+    std::lock_guard<std::mutex> hold(g_memory_lock);
+    g_allocations[*ptr] = {device, bytes};
+    g_in_use[device] += static_cast<int64_t>(bytes);
+    if (g_in_use[device] > g_peak[device]) g_peak[device] = g_in_use[device];
+    return e;
+}
+
+cudaError_t tracked_free(void *ptr) {
+    if (!ptr) return cudaSuccess;
+    {
+        std::lock_guard<std::mutex> hold(g_memory_lock);
+        const auto found = g_allocations.find(ptr);
+        if (found != g_allocations.end()) {
+            g_in_use[found->second.first] -= static_cast<int64_t>(found->second.second);
+            g_allocations.erase(found);
+        }
+    }
+    return cudaFree(ptr);
+}
 
 // 8 independent FMA chains per thread: the issue-rate ceiling of the FP32
 // pipe, used as the measured denominator of the march roofline (the driver's
@@ -41,6 +78,16 @@ ls200_status ls200_host_alloc(int64_t bytes, void **out) {
 ls200_status ls200_host_free(void *ptr) {
     return guard([&] {
         if (ptr) LS_CUDA(cudaFreeHost(ptr));
+    });
+}
+
+ls200_status ls200_memory_stats(int device, int64_t *in_use, int64_t *peak, int reset_peak) {
+    return guard([&] {
+        LS_REQUIRE(device >= 0 && device < kTrackedDevices, "device index out of range");
+        std::lock_guard<std::mutex> hold(g_memory_lock);
+        if (in_use) *in_use = g_in_use[device];
+        if (peak) *peak = g_peak[device];
+        if (reset_peak) g_peak[device] = g_in_use[device];
     });
 }
 

@@ -138,6 +138,7 @@ class CudaSession:
         _native.check(lib.ls200_context_create(int(device_id), ctypes.byref(handle)),
                       "CUDA session")
         self._ctx = handle
+        self.device_id = int(device_id)
         name = ctypes.create_string_buffer(256)
         major, minor, sms = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
         call("ls200_device_info", self._ctx, name, 256, ctypes.byref(major),

@@ -7,6 +7,7 @@ callback; the kernel is the sm_100a PSR kernel of ``libls200.so``.
 
 from __future__ import annotations
 
+import ctypes
 import threading
 import time
 from collections.abc import Callable
@@ -18,7 +19,49 @@ from ._native import CudaBackendError, call, pinned_empty
 from .contract import AZIMUTH_COUNT, PATCH_SIZE, projection_array
 from .lightmap_cuda import LightingContext, patch_elevations
 
-__all__ = ["PsrCudaSession", "PsrCudaPatchTimings", "CudaBackendError"]
+__all__ = ["PsrCudaSession", "PsrCudaPatchTimings", "CudaBackendError",
+           "reduce_sun_vectors_for_psr"]
+
+#: Viewpoints x azimuth bins of the reduction: the most vectors it keeps.
+MAX_REDUCED_VECTORS = 5 * AZIMUTH_COUNT
+
+
+def _validate_moon_vectors(vectors_m) -> np.ndarray:
+    values = np.ascontiguousarray(vectors_m, dtype=np.float64)
+    if (values.ndim != 2 or values.shape[1:] != (3,) or values.shape[0] == 0
+            or not np.all(np.isfinite(values))):
+        raise ValueError("Moon-ME vectors must be finite values shaped (time, 3)")
+    return values
+
+
+def reduce_vectors_on(context_handle, dem, sun_vectors_m) -> tuple[np.ndarray, np.ndarray]:
+    """The PSR vector reduction on an existing ls200 context (see
+    reduce_sun_vectors_for_psr)."""
+    vectors = _validate_moon_vectors(sun_vectors_m)
+    elevation = np.ascontiguousarray(dem.elevation_m, dtype=np.float32)
+    height, width = elevation.shape
+    indices = np.empty(MAX_REDUCED_VECTORS, dtype=np.int64)
+    kept = ctypes.c_int(0)
+    call("ls200_psr_reduce_vectors", context_handle, elevation, int(width), int(height),
+         np.ascontiguousarray(dem.geo_transform, dtype=np.float64),
+         projection_array(dem.projection), vectors, len(vectors), indices.ctypes.data,
+         ctypes.byref(kept))
+    indices = np.ascontiguousarray(indices[:kept.value])
+    return np.ascontiguousarray(vectors[indices]), indices
+
+
+def reduce_sun_vectors_for_psr(dem, sun_vectors_m, *,
+                               device_id: int = 0) -> tuple[np.ndarray, np.ndarray]:
+    """Drop-in for reduce_sun_vectors_for_psr (src/lunarscout/_numba_horizon/
+    psr.py:61-91), computed on the device: per viewpoint (the DEM's four
+    corner pixels and its centre pixel) and 0.25-deg azimuth bin the vector
+    with the highest elevation (first on ties), deduplicated in order of first
+    appearance.  Returns (float64 reduced vectors, int64 indices)."""
+    context = LightingContext(device_id)
+    try:
+        return reduce_vectors_on(context.handle, dem, sun_vectors_m)
+    finally:
+        context.close()
 
 
 @dataclass(frozen=True, slots=True)
@@ -57,6 +100,11 @@ class PsrCudaSession:
             self.close()
         except Exception:
             pass
+
+    def reduce_sun_vectors(self, dem, sun_vectors_m) -> tuple[np.ndarray, np.ndarray]:
+        """reduce_sun_vectors_for_psr on this session's device."""
+        with self._lock, self._context.lock:
+            return reduce_vectors_on(self._context.handle, dem, sun_vectors_m)
 
     def allocate_pinned_horizon_buffer(self) -> np.ndarray:
         """Page-locked float32 (128, 128, 1440) buffer for direct decode + H2D."""

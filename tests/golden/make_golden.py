@@ -447,6 +447,31 @@ def codec_reference() -> None:
     )
 
 
+def psr_reduction_reference() -> None:
+    """The reference's reduce_sun_vectors_for_psr on long vector tables: one
+    year hourly on the 512 x 512 synthetic site, and three years hourly on the
+    4096 x 4096 site-scale DEM (only its five viewpoint elevations matter)."""
+    sys.path.insert(0, str(OUT.parents[1]))
+    from lunarscout._numba_horizon.geometry import DemGrid, ProjectionParameters
+    from lunarscout._numba_horizon.psr import reduce_sun_vectors_for_psr
+    from lunarscout_b200 import synthetic
+
+    cases = {
+        "plain_year": (synthetic.config1_dem(),
+                       synthetic.hours_between("2030-01-01T00", "2031-01-01T00", 1.0)),
+        "site_three_years": (synthetic.site_dem(),
+                             synthetic.hours_between("2030-01-01T00", "2033-01-01T00", 1.0)),
+    }
+    arrays = {}
+    for name, (ours, hours) in cases.items():
+        dem = DemGrid(ours.elevation_m, ours.geo_transform,
+                      ProjectionParameters.from_array(ours.projection.as_array()))
+        _, indices = reduce_sun_vectors_for_psr(dem, synthetic.sun_vectors(hours))
+        arrays[f"{name}_hours"] = np.array([hours[0], hours[-1], hours[1] - hours[0]])
+        arrays[f"{name}_indices"] = indices.astype(np.int64)
+    np.savez_compressed(OUT / "psr_reduction_reference.npz", **arrays)
+
+
 def main() -> None:
     parser = argparse.ArgumentParser()
     parser.add_argument("--simulate", action="store_true")
@@ -461,6 +486,7 @@ def main() -> None:
         "lighting_reference": lighting_reference,
         "codec": codec_reference,
         "safe_haven": safe_haven_reference,
+        "psr_reduction": psr_reduction_reference,
     }
     for name, job in jobs.items():
         if args.only and name not in args.only.split(","):

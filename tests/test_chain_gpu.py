@@ -85,7 +85,7 @@ def test_chain_products_equal_the_per_patch_sessions(chain_case):
     try:
         fractions = chain.sun_fractions(batch, sun).cpu().numpy()
         encoded = chain.sun_fraction_bytes(batch, sun).cpu().numpy()
-        psr = chain.psr(batch, sun)
+        psr = chain.psr(batch, sun, reduce=False)
         missions = chain.mission_durations(batch, sun, sample_hours=sample_hours,
                                            start_windows=windows, earth_vectors_m=earth)
         havens = chain.safe_haven(batch, sun, earth, month_index_of=months,
@@ -118,6 +118,33 @@ def test_chain_products_equal_the_per_patch_sessions(chain_case):
     finally:
         lighting.close()
         psr_session.close()
+
+
+def test_chain_psr_is_the_reference_product_on_the_oracle(chain_case):
+    """chain.psr reduces the vectors over the DEM (as the PSR pipeline does)
+    and evaluates every patch against them: equal to the oracle's reduction
+    followed by the oracle's PSR, outside the counted 1e-4 deg band around the
+    limb threshold."""
+    from oracle import products
+
+    chain, batch, dem = chain_case["chain"], chain_case["batch"], chain_case["dem"]
+    sun = chain_case["sun"]
+    reduced, indices = chain.reduced_sun_vectors(sun)
+    _, expected_indices = products.reduce_sun_vectors(dem, sun)
+    np.testing.assert_array_equal(indices, expected_indices)
+    np.testing.assert_array_equal(reduced, sun[expected_indices])
+    assert len(indices) < len(sun)
+    psr = chain.psr(batch, sun)
+    band_pixels = 0
+    for i, patch in enumerate(batch.patches):
+        horizons, tile = _host(batch, i), _tile(patch)
+        expected = products.psr_tile(dem, horizons, reduced, **tile)
+        peak = products.psr_peak_margin(dem, horizons, reduced, **tile)
+        band = np.abs(peak - products.PSR_LIMB_THRESHOLD) < 1e-4
+        band_pixels += int(band.sum())
+        assert not np.any((psr[i] != expected) & ~band), patch
+    assert any(np.any(p == 255) for p in psr)
+    assert band_pixels < 0.001 * sum(p.size for p in psr)
 
 
 def test_chain_validation(chain_case):

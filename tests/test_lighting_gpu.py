@@ -297,3 +297,23 @@ def test_earth_visibility_against_the_reference_cpu_margins(lighting_session, si
     # can flip only where its margin lies within that of the threshold.
     flips = np.count_nonzero(np.abs(golden["margins"]) <= MARGIN_TOL, axis=0)
     assert np.all(np.abs(got - expected) * len(golden["margins"]) <= flips + 1e-3)
+
+
+def test_device_psr_vector_reduction_equals_the_oracle(psr_session, site):
+    """The device reduction (ls200_psr_reduce_vectors) against the oracle on
+    the 125-step table and against the reference's own indices on one year
+    (8,761) and three years (26,305) of hourly vectors."""
+    from lunarscout_b200.psr_cuda import reduce_sun_vectors_for_psr
+    from test_oracle_lighting_pins import _reduction_cases
+
+    reduced, indices = psr_session.reduce_sun_vectors(site["dem"], site["sun"])
+    _, expected = products.reduce_sun_vectors(site["dem"], site["sun"])
+    np.testing.assert_array_equal(indices, expected)
+    np.testing.assert_array_equal(reduced, site["sun"][expected])
+    for name, dem, sun, expected in _reduction_cases():
+        _, indices = reduce_sun_vectors_for_psr(dem, sun)
+        np.testing.assert_array_equal(indices, expected, err_msg=name)
+    with pytest.raises(ValueError):
+        psr_session.reduce_sun_vectors(site["dem"], np.zeros((0, 3)))
+    with pytest.raises(ValueError):
+        psr_session.reduce_sun_vectors(site["dem"], np.full((4, 3), np.nan))

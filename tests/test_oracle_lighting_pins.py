@@ -164,3 +164,22 @@ def test_cbin_codec_matches_reference_encoder():
     decoded = products.decode_tile(payload)
     np.testing.assert_array_equal(decoded[[0, 5, 9, 777, 16383]], arrays["decoded_rows"])
     assert np.all(decoded[5, :7] == np.float32(-32767) * (np.float32(50.0) / np.float32(32767.0)))
+
+
+def _reduction_cases():
+    from lunarscout_b200 import synthetic
+
+    arrays = load_golden("psr_reduction_reference.npz")
+    dems = {"plain_year": synthetic.config1_dem, "site_three_years": synthetic.site_dem}
+    for name, make in dems.items():
+        first, last, step = arrays[f"{name}_hours"]
+        hours = np.arange(first, last + 0.5 * step, step)
+        yield name, make(), synthetic.sun_vectors(hours), arrays[f"{name}_indices"]
+
+
+def test_psr_vector_reduction_matches_reference_on_long_tables():
+    """One year hourly (8,761 vectors) and three years hourly (26,305
+    vectors) against the reference's own reduce_sun_vectors_for_psr."""
+    for name, dem, sun, expected in _reduction_cases():
+        _, indices = products.reduce_sun_vectors(dem, sun)
+        np.testing.assert_array_equal(indices, expected, err_msg=name)

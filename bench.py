@@ -587,11 +587,16 @@ def multisite_benchmark(session, stream, args, world, rank):
         elapsed = max_over_ranks(start.elapsed_time(end) / 1000.0, world)
         return world * timed_rays / elapsed, elapsed
 
-    tuned = tune_batch(session, warmup[:TUNE_TILES], device_out=outputs["ladder"].data_ptr(),
-                       azimuth_count=AZIMUTHS, traversal="ladder")
+    # Each batched traversal runs with the launch configuration the autotuner
+    # picks for it (the relative arithmetic holds more registers).
+    tuned = {traversal: tune_batch(session, warmup[:TUNE_TILES],
+                                   device_out=outputs[traversal].data_ptr(),
+                                   azimuth_count=AZIMUTHS, traversal=traversal)
+             for traversal in ("exact", "ladder", "relative-ladder")}
     values, seconds = {}, {}
     values["plain"], seconds["plain"] = timed(plain, outputs["exact"])
     for traversal in ("exact", "ladder", "relative-ladder"):
+        session.set_batch_config(tuned[traversal].best)
         values[traversal], seconds[traversal] = timed(batched(traversal), outputs[traversal])
     result = {
         "metric": "multi-site horizon rays/s (uneven batch, 2 DEM passes, 200 km)",
@@ -607,12 +612,14 @@ def multisite_benchmark(session, stream, args, world, rank):
         "batched_split_seconds": {
             traversal: {"segments_and_setup": split[0], "march": split[1]}
             for traversal, split in splits.items()},
-        "launch_config": {"lanes_per_azimuth": tuned.best.lanes_per_azimuth,
-                          "min_blocks": tuned.best.min_blocks,
-                          "tuned_on": f"{TUNE_TILES} tiles of the warm-up batch, ladder",
-                          "candidates_ms": {
-                              f"lanes{c.lanes_per_azimuth}/blocks{c.min_blocks}":
-                                  1000.0 * s for c, s in tuned.seconds.items()}},
+        "launch_config": {
+            traversal: {"lanes_per_azimuth": result.best.lanes_per_azimuth,
+                        "min_blocks": result.best.min_blocks,
+                        "candidates_ms": {
+                            f"lanes{c.lanes_per_azimuth}/blocks{c.min_blocks}": 1000.0 * t
+                            for c, t in result.seconds.items()}}
+            for traversal, result in tuned.items()},
+        "launch_config_tuned_on": f"{TUNE_TILES} tiles of the warm-up batch",
         "sites": SITES, "tiles_per_launch": SITES, "warmup_tiles": WARMUP_TILES,
         "rays_timed_per_rank": timed_rays,
         "rays": "rays of pixels inside each site DEM (partial edge tiles count their valid part)",
@@ -883,7 +890,7 @@ def adjoint_benchmark(session, args, rank):
     azimuths, 20 km rays, loss = weighted (uniform [0, 1], seeded) mean smooth
     sun fraction over 29.53 days at 2 h steps (355 times).  Times the forward
     (march with argmax checkpoints, sun directions, loss) and the adjoint, and
-    checks central finite differences at +-0.05 m on 200 cells."""
+    checks central finite differences (adjoint_finite_differences)."""
     import torch
 
     from lunarscout_b200.adjoint import SunLossProblem
@@ -922,36 +929,70 @@ def adjoint_benchmark(session, args, rank):
                  "fraction)",
     }
     if not args.skip_cpu:
-        problem.forward_value([heights])
-        problem.replay_value()
-        (grad,) = problem.backward_value(1.0)
-        grad = grad.cpu().numpy()
-        magnitude = np.abs(grad).ravel()
-        live = np.flatnonzero(magnitude > 1e-3 * magnitude.max())
-        cells = rng.choice(live, min(ADJOINT_FD_CELLS, live.size), replace=False)
-        observer = np.zeros(grad.shape, dtype=bool)
-        observer[896:1152, 896:1152] = True
+        result["finite_differences_fixed_sampling"] = adjoint_finite_differences(
+            problem, heights, dem, rng)
+    problem.close()
+    return result
+
+
+# Steps of the finite-difference check (m): the configured +-0.05 m, and two
+# powers of two a factor 4 apart for the Richardson extrapolation.
+FD_STEPS = (0.05, 2.0 ** -10, 2.0 ** -12)
+FD_STRONGEST = 50
+
+
+def adjoint_finite_differences(problem, heights, dem, rng):
+    """Central differences of the replayed loss (the march's sampling held
+    fixed) against the adjoint on ADJOINT_FD_CELLS random cells with a
+    gradient and the FD_STRONGEST largest-gradient cells, split into the
+    observers' own cells and terrain: at +-0.05 m, at 2^-12 m, and the
+    Richardson extrapolation (16 D(2^-12) - D(2^-10)) / 15.  Each difference
+    divides by the float32 heights' actual separation."""
+    problem.forward_value([heights])
+    problem.replay_value()
+    (grad,) = problem.backward_value(1.0)
+    grad = grad.cpu().numpy()
+    magnitude = np.abs(grad).ravel()
+    live = np.flatnonzero(magnitude > 1e-3 * magnitude.max())
+    picks = {"random": rng.choice(live, min(ADJOINT_FD_CELLS, live.size), replace=False),
+             "strongest": np.argsort(magnitude)[-FD_STRONGEST:]}
+    observer = np.zeros(grad.shape, dtype=bool)
+    observer[896:1152, 896:1152] = True
+
+    def difference(y, x, step):
+        h = heights.clone()
+        base = float(heights[y, x])
+        h[y, x] = base + step
+        upper = float(h[y, x])
+        plus = problem.replay_value([h])
+        h[y, x] = base - step
+        lower = float(h[y, x])
+        minus = problem.replay_value([h])
+        return (plus - minus) / (upper - lower)
+
+    summary = {}
+    for pick, cells in picks.items():
         errors = {"terrain": [], "observer": []}
         for index in cells:
             y, x = divmod(int(index), dem.width)
-            h = heights.clone()
-            h[y, x] += 0.05
-            plus = problem.replay_value([h])
-            h[y, x] -= 0.1
-            minus = problem.replay_value([h])
-            error = abs((plus - minus) / 0.1 - grad[y, x]) / abs(grad[y, x])
-            errors["observer" if observer[y, x] else "terrain"].append(error)
-        problem.set_heights([heights])
-        summary = {}
+            d = [difference(y, x, step) for step in FD_STEPS]
+            richardson = (16.0 * d[2] - d[1]) / 15.0
+            g = grad[y, x]
+            errors["observer" if observer[y, x] else "terrain"].append(
+                [abs(d[0] - g) / abs(g), abs(d[2] - g) / abs(g), abs(richardson - g) / abs(g)])
         for kind, values in errors.items():
-            if values:
-                v = np.array(values)
-                summary[kind] = {"cells": int(v.size), "median_rel": float(np.median(v)),
-                                 "p90_rel": float(np.quantile(v, 0.9)),
-                                 "within_1e-3": float(np.mean(v <= 1e-3))}
-        result["finite_differences_0.05m_fixed_sampling"] = summary
-    problem.close()
-    return result
+            if not values:
+                continue
+            v = np.array(values)
+            summary[f"{pick}_{kind}"] = {
+                "cells": int(len(v)),
+                "median_rel_0.05m": float(np.median(v[:, 0])),
+                "median_rel_2^-12m": float(np.median(v[:, 1])),
+                "median_rel_richardson": float(np.median(v[:, 2])),
+                "within_1e-3_richardson": float(np.mean(v[:, 2] <= 1e-3)),
+                "p90_rel_richardson": float(np.quantile(v[:, 2], 0.9))}
+    problem.set_heights([heights])
+    return summary
 
 
 SENSITIVITY_SIDE = 8192

@@ -141,6 +141,70 @@ def test_gradient_agrees_with_central_finite_differences(problem):
     assert np.mean(own_errors <= 1e-2) >= 0.8, own_errors
 
 
+def _central_difference(p, heights, y, x, step):
+    """Central difference of the replayed loss at cell (y, x), divided by the
+    float32 heights' actual separation (a step the heights cannot hold
+    exactly would otherwise bias the quotient)."""
+    h = heights.clone()
+    base = float(heights[y, x])
+    h[y, x] = base + step
+    upper = float(h[y, x])
+    plus = p.replay_value([h])
+    h[y, x] = base - step
+    lower = float(h[y, x])
+    minus = p.replay_value([h])
+    return (plus - minus) / (upper - lower)
+
+
+STEPS = (2.0 ** -4, 2.0 ** -6, 2.0 ** -8, 2.0 ** -10, 2.0 ** -12)
+
+
+def _sweep(p, heights, grad, cells, steps=STEPS):
+    """Relative error of the central difference at every step of `steps` and
+    of the Richardson extrapolation of the two smallest (steps a factor 4
+    apart: (16 D(s / 4) - D(s)) / 15 cancels the s^2 term)."""
+    raw = np.zeros((len(cells), len(steps)))
+    extrapolated = np.zeros(len(cells))
+    for i, index in enumerate(cells):
+        y, x = divmod(int(index), grad.shape[1])
+        d = [_central_difference(p, heights, y, x, step) for step in steps]
+        raw[i] = [abs(v - grad[y, x]) / abs(grad[y, x]) for v in d]
+        extrapolated[i] = abs((16.0 * d[-1] - d[-2]) / 15.0 - grad[y, x]) / abs(grad[y, x])
+    p.set_heights([heights])
+    return raw, extrapolated
+
+
+def test_observer_cell_differences_converge_to_the_gradient(problem):
+    """An observer's own cell moves every one of its rays at once, and a
+    near-field sample 1 m away turns a height change of s metres into an
+    elevation change of about s radians: at +-0.05 m that is ~3 deg, ten disk
+    radii, so the loss is far from linear over the step.  Shrinking the step
+    shows the central differences converging to the adjoint (error ~ s^2),
+    and the Richardson extrapolation of the two smallest steps agrees to
+    1e-3 in the median, on the observer cells with the largest gradients and
+    on 200 random cells with a gradient (observers and terrain)."""
+    p, dem, heights, _ = problem
+    p.forward_value([heights])
+    p.replay_value()
+    (grad,) = p.backward_value(1.0)
+    grad = grad.cpu().numpy()
+    magnitude = np.abs(grad)
+    live = magnitude > 1e-3 * magnitude.max()
+    observer = np.zeros_like(live)
+    observer[OBSERVERS] = True
+    own = np.flatnonzero((observer & live).ravel())
+    strongest_own = own[np.argsort(magnitude.ravel()[own])[-24:]]
+    raw, extrapolated = _sweep(p, heights, grad, strongest_own)
+    medians = np.median(raw, axis=0)
+    assert medians[-1] < medians[0] / 20.0, medians          # converging with the step
+    assert np.median(extrapolated) <= 1e-3, (medians, extrapolated)
+    rng = np.random.default_rng(25)
+    random_cells = rng.choice(np.flatnonzero(live.ravel()), 200, replace=False)
+    _, extrapolated = _sweep(p, heights, grad, random_cells, STEPS[-2:])
+    assert np.median(extrapolated) <= 1e-3, np.median(extrapolated)
+    assert np.mean(extrapolated <= 1e-2) >= 0.9, np.mean(extrapolated <= 1e-2)
+
+
 def test_full_march_finite_differences_are_reported(problem):
     """Through the full march a 5 cm change also moves step positions and can
     switch the winning sample; those differences are measured, not gated

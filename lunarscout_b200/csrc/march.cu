@@ -41,8 +41,15 @@ struct SharedLevels {
     __device__ __forceinline__ int4 cells(int l) const { return t.cells[l]; }
 };
 
+// Resident 128-thread blocks per SM the register budget is sized for (8:
+// 64 registers).
+#ifndef LS_MARCH_MIN_BLOCKS
+#define LS_MARCH_MIN_BLOCKS 8
+#endif
+
 template <bool kCount>
-__global__ void __launch_bounds__(128, 8) march_pass_kernel(const __grid_constant__ MarchParams P) {
+__global__ void __launch_bounds__(128, LS_MARCH_MIN_BLOCKS)
+    march_pass_kernel(const __grid_constant__ MarchParams P) {
     __shared__ LevelTable table;
     const float column_res = hypot_fused(P.m6, P.m9);
     const float resolution = mean_resolution(P.m6, P.m7, P.m9, P.m10);

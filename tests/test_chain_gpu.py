@@ -147,6 +147,41 @@ def test_chain_psr_is_the_reference_product_on_the_oracle(chain_case):
     assert band_pixels < 0.001 * sum(p.size for p in psr)
 
 
+def test_chain_lighting_products_match_the_oracle(chain_case):
+    """The chain's sun fractions, Earth-visibility fractions and Sun-only
+    mission durations on its resident horizons against the CPU oracle fed the
+    same horizons: fractions within 1e-4, visibility exact except where a
+    margin sits within 1e-4 deg of the threshold, durations exact except at
+    pixels where a fraction sits within 1e-4 of the 0.5 threshold."""
+    from oracle import products
+
+    chain, batch, dem = chain_case["chain"], chain_case["batch"], chain_case["dem"]
+    sun, earth, hours = chain_case["sun"], chain_case["earth"], chain_case["hours"]
+    fractions = chain.sun_fractions(batch, sun).cpu().numpy()
+    visible = chain.earth_visibility(batch, earth)
+    sample_hours = np.full(len(hours), 6.0)
+    windows = np.array([[0, 40], [40, 100], [100, len(hours)]], dtype=np.int32)
+    missions = chain.mission_durations(batch, sun, sample_hours=sample_hours,
+                                       start_windows=windows)
+    accepts = np.zeros((len(windows), len(hours)), dtype=bool)
+    for i, (start, stop) in enumerate(windows):
+        accepts[i, start:stop] = True
+    for i, patch in enumerate(batch.patches[:2]):
+        horizons, tile = _host(batch, i), _tile(patch)
+        h, w = patch.height, patch.width
+        expected = products.lighting_tiles(dem, horizons, sun, **tile)
+        got = fractions[i].reshape(len(sun), 128, 128)[:, :h, :w]
+        assert np.abs(got - expected).max() <= 1e-4
+        margins = products.lighting_tiles(dem, horizons, earth, margin=True, **tile)
+        near = np.any(np.abs(margins) < 1e-4, axis=0)
+        expected_visible = products.earth_visibility(margins)
+        assert not np.any((visible[i] != expected_visible) & ~near)
+        expected_mission = products.longest_duration(expected >= np.float32(0.5),
+                                                     sample_hours, accepts)
+        edge = np.any(np.abs(expected - 0.5) < 1e-4, axis=0)
+        assert not np.any((missions[i] != expected_mission) & ~edge[None])
+
+
 def test_chain_validation(chain_case):
     from lunarscout_b200.chain import ProductChain
 

@@ -1558,8 +1558,9 @@ def run_profile_case():
 
 
 def run_profile_multisite():
-    """Four tiles of the multi-site batch through the persistent march, exact
-    traversal then skip ladder (launches 2 and 4 are the marches); used under
+    """Four tiles of the multi-site batch through the persistent march: the
+    reference traversal, the skip ladder, then the skip ladder in the
+    relative arithmetic (march_sites_kernel launches 0, 1, 2); used under
     ncu, never timed."""
     import torch
 
@@ -1578,7 +1579,7 @@ def run_profile_multisite():
                               (grid.height // 2 // TILE) * TILE, RANGE_M, OBSERVER_M))
     out = torch.empty(len(tiles) * RAYS_PER_TILE, dtype=torch.float32, device="cuda")
     torch.cuda.synchronize()
-    for traversal in ("exact", "ladder"):
+    for traversal in ("exact", "ladder", "relative-ladder"):
         session.march_sites(tiles, device_out=out.data_ptr(), azimuth_count=AZIMUTHS,
                             traversal=traversal, degrees=True)
     session.close()
@@ -1610,7 +1611,7 @@ def main():
     parser.add_argument("--profile", nargs="?", const="site", choices=("site", "multisite"),
                         help="small profiling case, no timing: 'site' = one site-scale tile "
                              "(two march steps, two lighting launches); 'multisite' = four "
-                             "tiles through the persistent march (exact, then ladder)")
+                             "tiles through the persistent march (exact, ladder, relative ladder)")
     args = parser.parse_args()
     if args.warmup < 3:
         args.warmup = 3

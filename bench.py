@@ -1079,10 +1079,11 @@ def sensitivity_benchmark(session, regional, args, rank):
     psr_s = timed(lambda: psr_launch(reduced_table, psr))
     psr_all_s = timed(lambda: psr_launch(table, psr_all))
     # Sun + Earth mission duration: condition = fraction >= 0.5 and Earth
-    # margin >= 0, weekly candidate start windows, 1 h samples.
-    week = 7 * 24
-    starts = np.arange(0, SENSITIVITY_STEPS - week, week, dtype=np.int32)
-    start_windows = np.ascontiguousarray(np.stack([starts, starts + week], axis=1))
+    # margin >= 0, 30-day candidate start windows (36 over the three years;
+    # the device reducer takes up to 64), 1 h samples.
+    window = 30 * 24
+    starts = np.arange(0, SENSITIVITY_STEPS - window, window, dtype=np.int32)
+    start_windows = np.ascontiguousarray(np.stack([starts, starts + window], axis=1))
     sample_hours = np.ones(SENSITIVITY_STEPS, dtype=np.float64)
     mission = torch.empty((count, len(starts), plane), dtype=torch.float32, device="cuda")
 
@@ -1136,7 +1137,7 @@ def sensitivity_benchmark(session, regional, args, rank):
         "psr_fraction": float((masks > 0).mean()),
         "psr_fraction_all_vectors": float((psr_all.cpu().numpy() > 0).mean()),
         "psr_band": band,
-        "mission_sun_earth": {"windows": int(len(starts)), "window_hours": week,
+        "mission_sun_earth": {"windows": int(len(starts)), "window_hours": window,
                               "px_steps_per_s": count * plane * SENSITIVITY_STEPS / mission_s,
                               "seconds": mission_s,
                               "mean_longest_hours": float(mission.mean())},
@@ -1287,30 +1288,51 @@ def run_ours(args):
     e2e_session.close()
     del host_segments
 
+    def leg(name, run):
+        """One secondary leg; on one GPU a failure is recorded in its field
+        (the headline line still prints), with more ranks it propagates so
+        that no rank is left waiting in a collective."""
+        started = time.perf_counter()
+        try:
+            result = run()
+        except Exception as error:
+            if world > 1:
+                raise
+            import traceback
+
+            traceback.print_exc()
+            result = {"error": f"{type(error).__name__}: {error}"[:500]}
+        log(f"[bench] {name} leg in {time.perf_counter() - started:.1f}s: "
+            f"{json.dumps(result)[:2000]}")
+        return result
+
     parity = None
     if rank == 0 and world == 1 and not args.skip_cpu:
-        parity = site_parity(session, dems, primary, regional, segments[args.warmup],
-                             tiles[args.warmup])
+        parity = leg("parity", lambda: site_parity(session, dems, primary, regional,
+                                                    segments[args.warmup], tiles[args.warmup]))
     numba_reference = None
     if rank == 0 and world == 1 and not args.skip_reference_numba:
         tile_row, tile_column = tiles[args.warmup]
         step(args.warmup)
         torch.cuda.synchronize()
-        numba_reference = reference_numba_cuda(primary, regional, segments[args.warmup],
-                                               tiles[args.warmup], output.cpu().numpy())
+        numba_reference = leg("reference_numba_cuda", lambda: reference_numba_cuda(
+            primary, regional, segments[args.warmup], tiles[args.warmup],
+            output.cpu().numpy()))
         numba_reference["ours_rays_per_s_device"] = value
         numba_reference["ours_rays_per_s_e2e"] = e2e_value
 
-    lighting = lighting_benchmark(session, dems, segments, tiles, primary, args, world, rank)
+    lighting = leg("lightmap", lambda: lighting_benchmark(session, dems, segments, tiles,
+                                                          primary, args, world, rank))
     del segments
-    multisite = None if args.skip_multisite else multisite_benchmark(session, stream, args,
-                                                                     world, rank)
-    adjoint = None if args.skip_adjoint else adjoint_benchmark(session, args, rank)
-    sensitivity = (None if args.skip_sensitivity or world > 1
-                   else sensitivity_benchmark(session, regional, args, rank))
+    multisite = None if args.skip_multisite else leg(
+        "multisite", lambda: multisite_benchmark(session, stream, args, world, rank))
+    adjoint = None if args.skip_adjoint else leg(
+        "adjoint", lambda: adjoint_benchmark(session, args, rank))
+    sensitivity = (None if args.skip_sensitivity or world > 1 else leg(
+        "sensitivity", lambda: sensitivity_benchmark(session, regional, args, rank)))
     # The public generator runs on device 0 (as the reference's does): 1 GPU only.
-    generate = (None if args.skip_generate or world > 1
-                else generate_benchmark(primary, regional, rank))
+    generate = (None if args.skip_generate or world > 1 else leg(
+        "generate_horizons", lambda: generate_benchmark(primary, regional, rank)))
 
     fp32_peak = session.fp32_probe()
     pass_times = np.array(pass_times)

@@ -74,7 +74,7 @@ class ProductChain:
         self.session = CudaSession(device_id)
         self.dems = list(dems)
         self.primary = self.dems[0]
-        self.device_dems = [self.session.upload_pyramid(self.session.build_max_pyramid(dem))
+        self.device_dems = [self.session.upload_pyramid(self.session.build_max_pyramid(dem), dem)
                             for dem in self.dems]
         self.maximum_distance_m = float(maximum_distance_m)
         self.observer_elevation_m = float(observer_elevation_m)

@@ -10,10 +10,13 @@
 // so every written multiply and add rounds separately, and the multiply-adds
 // that the reference's GPU compiler fuses are written as explicit __fmaf_rn:
 //   * every "x + a*b" / "x - a*b" whose product feeds the add is fused;
-//   * for "a*b + c*d" the first product is fused.
-// Division, reciprocal and square root are IEEE round-to-nearest.  With the
-// same segment inputs the results are bit-identical to the CPU oracle's FP32
-// restatement, which reproduces the reference's golden traversal captures.
+//   * for "a*b + c*d" the first product is fused, except local_x^2 =
+//     dist*dist - local_z^2, which fuses local_z^2.
+// That is the reference's Numba-CUDA kernel as NVVM compiles it on the B200
+// (its slopes on the same GPU are the golden file numba_cuda_b200.npz of the
+// tests).  Division, reciprocal and square root are IEEE round-to-nearest.
+// With the same segment inputs the results are bit-identical to the CPU
+// oracle's FP32 restatement under its production mask.
 //
 // The march is bound by instruction issue (its gathers hit L1/L2), so the
 // work per node visit is kept small without changing any rounded value or
@@ -217,14 +220,15 @@ __device__ __forceinline__ float above_slope(float dist, float above, float radi
     radius_sum = __fadd_rn(radius_sum, observer_z);
     const float numerator = __fmaf_rn(above, radius_sum, -squared);
     const float local_z = __fdiv_rn(numerator, __fmul_rn(2.0f, observer_radius));
-    const float lx2 = __fmaf_rn(dist, dist, -__fmul_rn(local_z, local_z));
+    const float lx2 = __fmaf_rn(-local_z, local_z, squared);
     const float local_x = lx2 > 0.0f ? __fsqrt_rn(lx2) : 1e-6f;
     return __fdiv_rn(local_z, local_x);
 }
 
 // Local-z slope of a terrain point seen over the chord `dist`
 // (cuda_backend.py:812-830): numerator fused on its first product, local_x^2
-// fused on dist*dist.
+// = dist*dist - local_z^2 fused on local_z*local_z (dist*dist rounded), as
+// the reference's Numba-CUDA kernel computes it on the B200.
 __device__ __forceinline__ float sample_slope(float dist, float height, float radius,
                                               float observer_radius) {
     const float squared = __fmul_rn(dist, dist);
@@ -233,7 +237,7 @@ __device__ __forceinline__ float sample_slope(float dist, float height, float ra
     const float radius_sum = __fadd_rn(point_radius, observer_radius);
     const float numerator = __fmaf_rn(radius_delta, radius_sum, -squared);
     const float local_z = __fdiv_rn(numerator, __fmul_rn(2.0f, observer_radius));
-    const float lx2 = __fmaf_rn(dist, dist, -__fmul_rn(local_z, local_z));
+    const float lx2 = __fmaf_rn(-local_z, local_z, squared);
     const float local_x = lx2 > 0.0f ? __fsqrt_rn(lx2) : 1e-6f;
     return __fdiv_rn(local_z, local_x);
 }
@@ -247,7 +251,7 @@ __device__ __forceinline__ float bound_slope(float dist, float height, float rad
     radius_sum = __fadd_rn(radius_sum, observer_z);
     const float numerator = __fmaf_rn(height_delta, radius_sum, -squared);
     const float local_z = __fdiv_rn(numerator, __fmul_rn(2.0f, observer_radius));
-    const float lx2 = __fmaf_rn(dist, dist, -__fmul_rn(local_z, local_z));
+    const float lx2 = __fmaf_rn(-local_z, local_z, squared);
     const float local_x = lx2 > 0.0f ? __fsqrt_rn(lx2) : 1e-6f;
     return __fdiv_rn(local_z, local_x);
 }

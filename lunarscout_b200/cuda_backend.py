@@ -208,8 +208,19 @@ class CudaSession:
         self._dems.add(dem)
         return dem
 
-    def upload_pyramid(self, pyramid) -> DeviceDem:
+    def upload_pyramid(self, pyramid, dem=None) -> DeviceDem:
+        """Upload a PyramidArrays (level 0 + mips).  A pyramid carries its
+        georeference only as float32 map and projection parameters, which is
+        enough for the march; segment fitting needs the float64
+        geotransform and projection, so callers that fit segments on the
+        device pass the DemGrid the pyramid was built from (float32 rounds
+        the polar latitude origin past -pi/2 and moves the observers)."""
         geo, proj, mp = _pyramid_geo(pyramid)
+        if dem is not None:
+            from .contract import projection_array
+
+            geo = np.ascontiguousarray(dem.geo_transform, dtype=np.float64)
+            proj = projection_array(dem.projection)
         mips = np.ascontiguousarray(pyramid.mips, dtype=np.float32)
         return self.upload_dem(pyramid.level0, geo, proj, mp, mips if mips.size else None)
 

@@ -64,7 +64,8 @@ class HorizonTileGenerator:
             if pyramids is None:
                 pyramids = [self.session.build_max_pyramid(dem) for dem in dems]
             self.pyramids = tuple(pyramids)
-            self.device_dems = [self.session.upload_pyramid(p) for p in self.pyramids]
+            self.device_dems = [self.session.upload_pyramid(p, dem)
+                                for p, dem in zip(self.pyramids, dems)]
         except BaseException:
             self.close()
             raise
@@ -142,7 +143,7 @@ class BatchedTileGenerator:
         self.session = session
         if pyramids is None:
             pyramids = [session.build_max_pyramid(dem) for dem in dems]
-        self.device_dems = [session.upload_pyramid(p) for p in pyramids]
+        self.device_dems = [session.upload_pyramid(p, dem) for p, dem in zip(pyramids, dems)]
         self.primary = dems[0]
         self.patches = list(patches)
         self.position = {(p.tile_x, p.tile_y): i for i, p in enumerate(self.patches)}

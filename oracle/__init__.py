@@ -76,12 +76,18 @@ def ladder_mask(cap: int = 0, min_km: int = 0, base: int | None = None) -> int:
         raise ValueError("ladder cap and distance must be between 0 and 15")
     return (PRODUCTION_MASK if base is None else base) | OPT_LADDER | (cap << 24) | (min_km << 28)
 
-#: Contraction mask whose FP32 arithmetic reproduces the reference's golden
-#: production captures (tests/test_oracle_pins.py checks it).
-PRODUCTION_MASK = (
+#: Contraction mask whose FP32 arithmetic reproduces the golden captures of
+#: the reference's C# production kernel (tests/test_oracle_pins.py checks it):
+#: local_x^2 = dist * dist - local_z^2 fuses dist * dist.
+CSHARP_MASK = (
     CF_EVAL | CF_TAN | CF_PLANAR | CF_CHORD | CF_CHORD_ALT | CF_TRUEM | CF_NEAR
     | CF_BOUND | CF_SLOPE | CF_MAG | CF_BILIN | CF_RES | CF_LXS_ALT | CF_SHIFT
 )
+#: The reference's runtime arithmetic: its Numba-CUDA kernel
+#: (cuda_backend.py:656-1134) as NVVM compiles it, run on a B200; the same as
+#: the C# captures except that local_x^2 fuses local_z * local_z (pinned by
+#: tests/golden/numba_cuda_b200.npz).  The product marches with it.
+PRODUCTION_MASK = CSHARP_MASK & ~CF_LXS_ALT
 
 
 def build(force: bool = False) -> Path:

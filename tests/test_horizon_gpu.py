@@ -166,3 +166,16 @@ def test_degrees_conversion_matches_host_contract(cuda_session):
     expected = HorizonBuffers(slopes).degrees()
     assert np.isneginf(got[3, 5])
     np.testing.assert_allclose(got, expected, rtol=0, atol=1e-5)
+
+
+def test_device_march_reproduces_the_reference_numba_cuda_slopes(cuda_session):
+    """The drop-in on the same inputs as the reference's own Numba-CUDA
+    kernel run on a B200 (tests/golden/numba_cuda_b200.npz: two DEM passes,
+    16,384 pixels x 12 azimuths): every slope bit for bit."""
+    from test_oracle_pins import _numba_case
+
+    arrays, pyramids, common = _numba_case()
+    gpu, _ = cuda_session.subpatch_hierarchical_all_passes(
+        arrays["segments"], pyramids, tile_width=128, tile_height=128, subpatch_size=8,
+        **common)
+    np.testing.assert_array_equal(gpu, arrays["slopes"])

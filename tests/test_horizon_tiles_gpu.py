@@ -256,3 +256,27 @@ def test_batched_generation_writes_the_per_tile_bytes(tmp_path, synthetic_pair, 
     ladder = sorted((tmp_path / "ladder").rglob("horizon_*"))
     assert [p.name for p in ladder] == [p.name for p in plain]
     assert all(HorizonTileStore.is_complete(p) for p in ladder)
+
+
+def test_generator_tiles_fit_segments_on_the_float64_georeference(synthetic_pair, cuda_session):
+    """The public generator uploads pyramids (whose georeference is float32)
+    but fits segments with each DEM's float64 geotransform and projection:
+    its tiles equal the device path fed the DemGrids themselves.  In float32
+    the polar latitude origin -pi/2 rounds past the pole and moves the
+    observers; at 1.5 m above the terrain that changed horizons by degrees."""
+    from lunarscout_b200.horizon import HorizonTileGenerator
+
+    primary, regional = synthetic_pair
+    dems = [cuda_session.upload_dem_grid(primary), cuda_session.upload_dem_grid(regional)]
+    tile = dict(tile_column=128, tile_row=128, tile_width=128, subpatch_size=8)
+    with HorizonTileGenerator([primary, regional], session=cuda_session) as generator:
+        got = generator.degrees(128, 128, observer_elevation_m=1.5, maximum_distance_m=100_000.0)
+    segments = cuda_session.generate_segments(dems, azimuth_count=AZ,
+                                              maximum_distance_m=100_000.0,
+                                              observer_elevation_m=1.5, **tile)
+    pyramids = [cuda_session.build_max_pyramid(primary), cuda_session.build_max_pyramid(regional)]
+    slopes, _ = cuda_session.subpatch_hierarchical_all_passes(
+        segments, pyramids, tile_height=128, observer_elevation_m=1.5, **tile)
+    np.testing.assert_array_equal(got, cuda_session.slopes_to_degrees(slopes))
+    for dem in dems:
+        dem.close()

@@ -16,6 +16,7 @@ from conftest import load_golden
 
 CAP = oracle.OPT_EXIT_CAP
 PROD = oracle.PRODUCTION_MASK
+CSHARP = oracle.CSHARP_MASK
 
 
 def _interpolated(segments4, shifts=((4, 4), (-4, 4), (4, -4), (-4, -4))):
@@ -53,7 +54,7 @@ def test_oracle_reproduces_the_csharp_traversal_trace_exactly(production_case):
     seg = _interpolated(arrays["csharp_trace_segments"])
     value, trace = oracle.hierarchy_maximum(
         seg, pyramids[1], observer_z=float(arrays["csharp_trace_observer_z"]),
-        radius=1737400.0, resolution=30.0, pass_index=1, mask=PROD | CAP, capacity=4096)
+        radius=1737400.0, resolution=30.0, pass_index=1, mask=CSHARP | CAP, capacity=4096)
     expected = arrays["csharp_trace"]
     assert trace.shape == expected.shape == (932, 12)
     assert _same(trace, expected)
@@ -72,7 +73,7 @@ def test_oracle_reproduces_the_csharp_bilinear_boundary_trace(production_case):
     value, trace = oracle.hierarchy_maximum(
         seg, pyramid, observer_z=float(arrays["boundary_observer_z"]),
         radius=float(arrays["boundary_radius"]), resolution=float(arrays["boundary_resolution"]),
-        pass_index=0, mask=PROD | CAP, capacity=4096)
+        pass_index=0, mask=CSHARP | CAP, capacity=4096)
     expected = arrays["boundary_trace"]
     assert trace.shape == expected.shape
     # Structure and decisions exactly; values to the JSON's printed precision.
@@ -83,7 +84,7 @@ def test_oracle_reproduces_the_csharp_bilinear_boundary_trace(production_case):
 
 def test_oracle_with_the_superseded_cell_exit_cap_matches_csharp_per_dem_slopes(production_case):
     arrays, pyramids = production_case
-    got = _passes(arrays, pyramids, PROD | CAP)
+    got = _passes(arrays, pyramids, CSHARP | CAP)
     expected = arrays["csharp_per_dem_slopes"]
     np.testing.assert_allclose(got, expected, rtol=0, atol=3e-10)
 
@@ -198,3 +199,32 @@ def test_oracle_segments_match_reference_numba_and_csharp():
     # The reference's own C# tolerance (test_phase3_geometry.py:225).
     assert _path_error(got, arrays["csharp_segments"]) < 1e-5
     np.testing.assert_allclose(got, arrays["csharp_segments"], rtol=0, atol=1e-5)
+
+
+def _numba_case():
+    from lunarscout_b200 import synthetic
+    from lunarscout_b200.contract import PyramidArrays, map_parameters, projection_parameters
+
+    arrays = load_golden("numba_cuda_b200.npz")
+    pyramids = []
+    for dem in (synthetic.config1_dem(), synthetic.regional_dem()):
+        mips, levels = oracle.build_pyramid(dem.elevation_m)
+        pyramids.append(PyramidArrays(dem.elevation_m, mips, levels, map_parameters(dem),
+                                      projection_parameters(dem)))
+    column, row = (int(v) for v in arrays["tile"])
+    common = dict(tile_column=column, tile_row=row,
+                  observer_elevation_m=float(arrays["observer_elevation_m"]))
+    return arrays, pyramids, common
+
+
+def test_oracle_reproduces_the_reference_numba_cuda_march_on_the_b200():
+    """The reference's own Numba-CUDA kernel, run on a B200 (two DEM passes,
+    16,384 pixels x 12 azimuths): the production mask reproduces every slope
+    bit for bit; the C# captures' mask (local_x^2 fused on dist * dist) does
+    not."""
+    arrays, pyramids, common = _numba_case()
+    got, _ = oracle.march_all_passes(arrays["segments"], pyramids, **common)
+    np.testing.assert_array_equal(got, arrays["slopes"])
+    csharp, _ = oracle.march_all_passes(arrays["segments"], pyramids, mask=CSHARP, **common)
+    assert np.count_nonzero(csharp != arrays["slopes"]) > 0
+    assert np.isfinite(got).mean() > 0.99

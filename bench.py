@@ -475,33 +475,38 @@ SITES = 64
 WARMUP_TILES = 16  # the warm-up batch: one tile of each of the first 16 sites
 TUNE_TILES = 4
 MULTISITE_PARITY_RAYS = 20_000
-# The multi-site products run over this many of the batch's 64 tiles by
-# default (one lighting launch); --c3-full-lighting takes all 64.
-C3_LIGHT_TILES = 8
 
 
 def distance_over_every_ray(a, b, bin_deg=1e-5, bins=100_000):
     """p99.9 (to the histogram's bin width) and max of |a - b| (degrees) over
-    every finite ray of two degree batches [tiles, pixels, azimuths]; returns
-    also whether the -inf rays agree."""
+    every finite ray of two degree batches [tiles, pixels, azimuths], with
+    the (tile, pixel, azimuth) of the max, the rays beyond 0.01 and 1 deg,
+    and whether the -inf rays agree."""
     import torch
 
     counts = torch.zeros(bins + 1, dtype=torch.int64, device=a.device)
-    largest, same_inf, total = 0.0, True, 0
+    largest, at, same_inf, total, over = 0.0, None, True, 0, [0, 0]
     for t in range(a.shape[0]):
-        finite = torch.isfinite(a[t])
-        same_inf &= bool(torch.equal(finite, torch.isfinite(b[t])))
-        d = (a[t].double() - b[t].double())[finite & torch.isfinite(b[t])].abs()
+        finite = torch.isfinite(a[t]) & torch.isfinite(b[t])
+        same_inf &= bool(torch.equal(torch.isfinite(a[t]), torch.isfinite(b[t])))
+        full = torch.where(finite, (a[t].double() - b[t].double()).abs(),
+                           torch.zeros((), dtype=torch.float64, device=a.device))
+        d = full[finite]
         if d.numel() == 0:
             continue
         total += d.numel()
-        largest = max(largest, float(d.max()))
+        over[0] += int((d > 0.01).sum())
+        over[1] += int((d > 1.0).sum())
+        worst = int(torch.argmax(full))
+        if float(full.view(-1)[worst]) > largest:
+            largest = float(full.view(-1)[worst])
+            at = (t, worst // full.shape[1], worst % full.shape[1])
         counts += torch.bincount((d / bin_deg).long().clamp(max=bins), minlength=bins + 1)
     cumulative = torch.cumsum(counts, 0)
     rank = int(math.ceil(0.999 * int(cumulative[-1])))
     index = int(torch.searchsorted(cumulative, torch.tensor([rank], device=a.device)))
-    return {"p99.9": (index + 1) * bin_deg, "max": largest, "rays": total,
-            "inf_rays_agree": same_inf}
+    return {"p99.9": (index + 1) * bin_deg, "max": largest, "max_at": at, "rays": total,
+            "over_0.01": over[0], "over_1": over[1], "inf_rays_agree": same_inf}
 
 
 def multisite_benchmark(session, stream, args, world, rank):
@@ -631,12 +636,45 @@ def multisite_benchmark(session, stream, args, world, rank):
     }
     if rank == 0 and world == 1 and not args.skip_cpu:
         result["parity"] = multisite_parity(session, grids, regional, batch, outputs)
+        result["largest_distances_vs_fp64"] = {
+            name: ray_against_fp64(session, grids, regional, batch, outputs,
+                                   result["every_ray_vs_exact_deg"][name]["max_at"])
+            for name in ("ladder", "relative_ladder")}
     del outputs["exact"], outputs["ladder"]
     result["pipeline"] = multisite_products(session, stream, grids, batch,
                                             outputs["relative-ladder"], args)
     for dem in site_devs + [regional_dev]:
         dem.close()
     return result
+
+
+def ray_against_fp64(session, grids, regional, batch, outputs, at):
+    """Each traversal's degrees and the FP64 restatement's at one ray
+    (tile, pixel, azimuth) of the 64-site batch."""
+    import oracle
+    from lunarscout_b200.contract import PyramidArrays, map_parameters, projection_parameters
+
+    if at is None:
+        return None
+    t, pixel, azimuth = (int(v) for v in at)
+    tile, grid = batch[t], grids[t]
+    pyramids = []
+    for dem in (grid, regional):
+        mips, levels = oracle.build_pyramid(dem.elevation_m)
+        pyramids.append(PyramidArrays(dem.elevation_m, mips, levels, map_parameters(dem),
+                                      projection_parameters(dem)))
+    segments = session.generate_segments(list(tile.dems), tile_column=tile.tile_column,
+                                         tile_row=tile.tile_row, azimuth_count=AZIMUTHS,
+                                         maximum_distance_m=RANGE_M,
+                                         observer_elevation_m=OBSERVER_M)
+    fp64, _ = oracle.march_all_passes(segments, pyramids, tile_column=tile.tile_column,
+                                      tile_row=tile.tile_row, observer_elevation_m=OBSERVER_M,
+                                      pixels=np.array([pixel], np.int32),
+                                      azimuths=np.array([azimuth], np.int32), precision="f64")
+    values = {name: float(out[t, pixel, azimuth]) for name, out in outputs.items()}
+    values["fp64"] = float(np.degrees(np.arctan(fp64[0])))
+    values["ray"] = {"site": t, "pixel": pixel, "azimuth": azimuth}
+    return values
 
 
 def multisite_parity(session, grids, regional, batch, outputs):
@@ -706,10 +744,9 @@ def multisite_parity(session, grids, regional, batch, outputs):
 
 
 def multisite_products(session, stream, grids, batch, horizons, args):
-    """The multi-site products over two years of hourly steps (17,545) on the
-    first C3_LIGHT_TILES tiles of the 64-site batch (all 64 with
-    --c3-full-lighting), from the relative-ladder horizons left in HBM by the
-    batched march: sun-fraction bytes, PSR against each site's reduced Sun
+    """The multi-site products over two years of hourly steps (17,521) on the
+    64 tiles of the multi-site batch, from the relative-ladder horizons left in
+    HBM by the batched march: sun-fraction bytes, PSR against each site's reduced Sun
     vectors (the reduction over that site's DEM, on the device), and the
     Earth-visibility fraction.  The lightmap and PSR launches run eagerly and
     then as one replayed CUDA graph (one node per launch over the whole
@@ -724,7 +761,7 @@ def multisite_products(session, stream, grids, batch, horizons, args):
     from lunarscout_b200.lightmap_cuda import DeviceVectors
     from lunarscout_b200.psr_cuda import reduce_vectors_on
 
-    count = SITES if args.c3_full_lighting else C3_LIGHT_TILES
+    count = len(batch)
     plane = TILE * TILE
     hours = synthetic.hours_between("2030-01-01T00", "2032-01-01T00", 1.0)
     steps = len(hours)
@@ -1627,9 +1664,6 @@ def main():
                         help="leave out the 8192^2 streamed-adjoint sensitivity slice")
     parser.add_argument("--skip-reference-numba", action="store_true",
                         help="leave out the reference's own Numba-CUDA march on the same tile")
-    parser.add_argument("--c3-full-lighting", action="store_true",
-                        help="run the multi-site products over all 64 tiles of the batch "
-                             f"(default: the first {C3_LIGHT_TILES})")
     parser.add_argument("--profile", nargs="?", const="site", choices=("site", "multisite"),
                         help="small profiling case, no timing: 'site' = one site-scale tile "
                              "(two march steps, two lighting launches); 'multisite' = four "

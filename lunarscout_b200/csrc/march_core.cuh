@@ -623,18 +623,19 @@ __device__ __forceinline__ bool march_step_tracked(const Table &table, const Dem
         }
         // NaN fails every comparison, as the reference's isnan tests do.
         if (!(px >= 0.0f && py >= 0.0f && px < last_x && py < last_y)) return false;
-        if (!relative) {
-            rx = __fsub_rn(px, g.start_x);
-            ry = __fsub_rn(py, g.start_y);
-        }
-        const float planar_x = __fmul_rn(rx, resolution);
-        const float planar_y = __fmul_rn(ry, resolution);
-        const float planar_m = hypot_fused(planar_x, planar_y);
         const bool near = s < 0.5f;
         float true_m;
         if (near) {
             true_m = __fmul_rn(s, 1000.0f);
         } else {
+            // The planar distance only feeds the far-field chord.
+            if (!relative) {
+                rx = __fsub_rn(px, g.start_x);
+                ry = __fsub_rn(py, g.start_y);
+            }
+            const float planar_x = __fmul_rn(rx, resolution);
+            const float planar_y = __fmul_rn(ry, resolution);
+            const float planar_m = hypot_fused(planar_x, planar_y);
             const float pm2 = __fmul_rn(planar_m, planar_m);
             const float pm3 = __fmul_rn(pm2, planar_m);
             float chord = __fmaf_rn(g.c1, planar_m, __fmul_rn(g.c2, pm2));

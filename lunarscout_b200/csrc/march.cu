@@ -41,10 +41,11 @@ struct SharedLevels {
     __device__ __forceinline__ int4 cells(int l) const { return t.cells[l]; }
 };
 
-// Resident 128-thread blocks per SM the register budget is sized for (8:
-// 64 registers).
+// Resident 128-thread blocks per SM the register budget is sized for: 10
+// (51 registers, a few bytes of spills) marched 1-2 % faster than 8 (64
+// registers, none) with the 4-pixel lane layout; 12 was slower.
 #ifndef LS_MARCH_MIN_BLOCKS
-#define LS_MARCH_MIN_BLOCKS 8
+#define LS_MARCH_MIN_BLOCKS 10
 #endif
 // Adjacent pixels of one azimuth in a warp (a power of two up to 32); the
 // warp's other lanes take the next azimuths of the same pixels.  4 pixels x

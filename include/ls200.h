@@ -177,9 +177,8 @@ ls200_status ls200_march_sites(ls200_context *ctx, const ls200_site_tile *tiles,
 /* Launch configuration of ls200_march_sites for this context (results do
  * not depend on it): `lanes_per_azimuth` = how many adjacent pixels of one
  * azimuth a 32-ray warp job holds (a power of two from 1 to 32; the job then
- * spans 32 / lanes_per_azimuth azimuths), `min_blocks` = resident 128-thread blocks per SM, 10 (51
- * registers), 8 (64 registers) or 6 (80 registers).  Chosen by the
- * autotuner; defaults 2, 8. */
+ * spans 32 / lanes_per_azimuth azimuths), `min_blocks` = resident 128-thread blocks per SM, 8 (64
+ * registers) or 6 (80 registers).  Chosen by the autotuner; defaults 2, 8. */
 ls200_status ls200_set_batch_config(ls200_context *ctx, int lanes_per_azimuth, int min_blocks);
 ls200_status ls200_get_batch_config(ls200_context *ctx, int *lanes_per_azimuth, int *min_blocks);
 

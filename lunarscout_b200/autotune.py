@@ -21,7 +21,7 @@ from .cuda_backend import BatchConfig
 
 #: The default search space: lane layouts x occupancies, the default first.
 DEFAULT_CANDIDATES: tuple[BatchConfig, ...] = tuple(
-    BatchConfig(lanes, blocks) for lanes in (2, 1, 4, 8, 16, 32) for blocks in (8, 6, 10))
+    BatchConfig(lanes, blocks) for lanes in (2, 1, 4, 8, 16, 32) for blocks in (8, 6))
 
 
 @dataclass(frozen=True, slots=True)

@@ -17,8 +17,8 @@
 //
 // Launch configuration (autotuned, never changing results): how the 32 lanes
 // of a job map onto rays (L adjacent pixels x 32/L adjacent azimuths, L a
-// power of two up to 32), and the resident blocks per SM (10 at 51
-// registers, 8 at 64, 6 at 80).
+// power of two up to 32), and the resident blocks per SM (8 at 64 registers,
+// 6 at 80).
 #include "march_core.cuh"
 
 #include <map>
@@ -328,7 +328,6 @@ void march_sites_run(ls200_context *ctx, const ls200_site_tile *tiles, int tile_
         if (checkpoints) dispatch_argmax(ctx, P, traversal);
         else if (ctx->counting) dispatch<true, 8>(ctx, P, traversal);
         else if (ctx->batch_min_blocks == 6) dispatch<false, 6>(ctx, P, traversal);
-        else if (ctx->batch_min_blocks == 10) dispatch<false, 10>(ctx, P, traversal);
         else dispatch<false, 8>(ctx, P, traversal);
         if (seconds) LS_CUDA(cudaEventRecord(ctx->events[2], ctx->stream));
         // The host tables above must outlive their copies.
@@ -366,8 +365,7 @@ extern "C" ls200_status ls200_set_batch_config(ls200_context *ctx, int lanes_per
         LS_REQUIRE(lanes_per_azimuth >= 1 && lanes_per_azimuth <= 32 &&
                        (lanes_per_azimuth & (lanes_per_azimuth - 1)) == 0,
                    "lanes_per_azimuth must be a power of two from 1 to 32");
-        LS_REQUIRE(min_blocks == 6 || min_blocks == 8 || min_blocks == 10,
-                   "min_blocks must be 6, 8 or 10");
+        LS_REQUIRE(min_blocks == 6 || min_blocks == 8, "min_blocks must be 6 or 8");
         std::lock_guard<std::mutex> hold(ctx->lock);
         ctx->batch_lanes_per_azimuth = lanes_per_azimuth;
         ctx->batch_min_blocks = min_blocks;

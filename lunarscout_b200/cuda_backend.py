@@ -59,7 +59,7 @@ class BatchConfig:
     """Launch configuration of the persistent multi-site march:
     ``lanes_per_azimuth`` adjacent pixels of one azimuth per 32-ray warp job
     (a power of two up to 32; the job spans 32/lanes azimuths) and ``min_blocks``
-    resident 128-thread blocks per SM (10 at 51 registers, 8 at 64 or 6 at 80)."""
+    resident 128-thread blocks per SM (8 at 64 registers or 6 at 80)."""
 
     lanes_per_azimuth: int = 2
     min_blocks: int = 8

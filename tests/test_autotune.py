@@ -40,7 +40,7 @@ def test_default_candidates_are_valid_and_unique():
     assert len(set(DEFAULT_CANDIDATES)) == len(DEFAULT_CANDIDATES)
     for config in DEFAULT_CANDIDATES:
         assert config.lanes_per_azimuth in (32, 16, 8, 4, 2, 1)
-        assert config.min_blocks in (6, 8, 10)
+        assert config.min_blocks in (6, 8)
     assert DEFAULT_CANDIDATES[0] == BatchConfig()
 
 

@@ -15,6 +15,9 @@
 // That is the reference's Numba-CUDA kernel as NVVM compiles it on the B200
 // (its slopes on the same GPU are the golden file numba_cuda_b200.npz of the
 // tests).  Division, reciprocal and square root are IEEE round-to-nearest.
+// The x and y arithmetic of a step (path position and tangent, planar
+// offset, cell-exit slab) is issued as f32x2 pairs, whose lanes round as the
+// scalar intrinsics do.
 // With the same segment inputs the results are bit-identical to the CPU
 // oracle's FP32 restatement under its production mask.
 //
@@ -114,24 +117,38 @@ __device__ __forceinline__ float power_of_two(int shift) {
     return __int_as_float((127 + shift) << 23);
 }
 
-__device__ __forceinline__ float quartic(float x0, float a1, float a2, float a3, float a4,
-                                         float d) {
-    const float d2 = __fmul_rn(d, d);
-    const float d3 = __fmul_rn(d2, d);
-    const float d4 = __fmul_rn(d2, d2);
-    float r = __fmaf_rn(a1, d, x0);
-    r = __fmaf_rn(a2, d2, r);
-    r = __fmaf_rn(a3, d3, r);
-    return __fmaf_rn(a4, d4, r);
+// Two FP32 lanes per instruction (the f32x2 operations of sm_100): each
+// lane rounds exactly as the scalar __fadd_rn / __fmul_rn / __fmaf_rn does, so
+// the march pairs its x and y arithmetic without changing a bit.
+__device__ __forceinline__ float2 pair(float x, float y) { return make_float2(x, y); }
+__device__ __forceinline__ float2 sub2(float2 a, float2 b) {
+    float2 d;
+    asm("sub.rn.f32x2 %0, %1, %2;"
+        : "=l"(reinterpret_cast<unsigned long long &>(d))
+        : "l"(reinterpret_cast<const unsigned long long &>(a)),
+          "l"(reinterpret_cast<const unsigned long long &>(b)));
+    return d;
 }
 
-__device__ __forceinline__ float quartic_tangent(float a1, float a2, float a3, float a4,
-                                                 float d) {
-    const float d2 = __fmul_rn(d, d);
-    const float d3 = __fmul_rn(d2, d);
-    float r = __fmaf_rn(__fmul_rn(2.0f, a2), d, a1);
-    r = __fmaf_rn(__fmul_rn(3.0f, a3), d2, r);
-    return __fmaf_rn(__fmul_rn(4.0f, a4), d3, r);
+// The quartic path polynomial of both axes at once: lane x with
+// (start_x, a1..a4), lane y with (start_y, b1..b4); d2, d3, d4 are the powers
+// of the path offset d (cuda_backend.py:62-73).
+__device__ __forceinline__ float2 quartic2(float2 x0, float2 k1, float2 k2, float2 k3,
+                                           float2 k4, float2 d, float2 d2, float2 d3,
+                                           float2 d4) {
+    float2 r = __ffma2_rn(k1, d, x0);
+    r = __ffma2_rn(k2, d2, r);
+    r = __ffma2_rn(k3, d3, r);
+    return __ffma2_rn(k4, d4, r);
+}
+
+// Its derivative: a1 + 2 a2 d + 3 a3 d^2 + 4 a4 d^3 per lane
+// (cuda_backend.py:76-84).
+__device__ __forceinline__ float2 quartic_tangent2(float2 k1, float2 k2, float2 k3, float2 k4,
+                                                   float2 d, float2 d2, float2 d3) {
+    float2 r = __ffma2_rn(__fmul2_rn(pair(2.0f, 2.0f), k2), d, k1);
+    r = __ffma2_rn(__fmul2_rn(pair(3.0f, 3.0f), k3), d2, r);
+    return __ffma2_rn(__fmul2_rn(pair(4.0f, 4.0f), k4), d3, r);
 }
 
 // Clamped bilinear sample of sanitized level-0 cells; -32000 when any corner
@@ -338,12 +355,12 @@ __device__ __forceinline__ float cell_exit_advance(int shift, int cx, int cy, fl
                                                    int origin_x, int origin_y, float inv_x,
                                                    float inv_y, float fallback) {
     const float scale_f = power_of_two(shift);
-    const float min_x = static_cast<float>((cx << shift) - origin_x);
-    const float min_y = static_cast<float>((cy << shift) - origin_y);
-    const float edge_x = inv_x > 0.0f ? __fadd_rn(min_x, scale_f) : min_x;
-    const float edge_y = inv_y > 0.0f ? __fadd_rn(min_y, scale_f) : min_y;
-    const float tmx = __fmul_rn(__fsub_rn(edge_x, ux), inv_x);
-    const float tmy = __fmul_rn(__fsub_rn(edge_y, uy), inv_y);
+    const float2 low = pair(static_cast<float>((cx << shift) - origin_x),
+                            static_cast<float>((cy << shift) - origin_y));
+    const float2 high = __fadd2_rn(low, pair(scale_f, scale_f));
+    const float2 edge = pair(inv_x > 0.0f ? high.x : low.x, inv_y > 0.0f ? high.y : low.y);
+    const float2 tm = __fmul2_rn(sub2(edge, pair(ux, uy)), pair(inv_x, inv_y));
+    const float tmx = tm.x, tmy = tm.y;
     const float exit_distance = tmx < tmy ? tmx : tmy;
     const float to_exit = exit_distance > 0.0f ? exit_distance : fallback;
     return to_exit > 0.0f ? __fadd_rn(to_exit, 0.0001f) : fallback;
@@ -449,7 +466,8 @@ __device__ __forceinline__ float ladder_advance(const Table &table, const float 
 // With the relative arithmetic start_x, start_y are relative to the integer
 // origin (origin_x, origin_y); otherwise the origin is 0.
 struct RaySegment {
-    float start_x, start_y, a1, a2, a3, a4, b1, b2, b3, b4;
+    float2 start;           // (start_x, start_y)
+    float2 k1, k2, k3, k4;  // (a1, b1) .. (a4, b4)
     float s_start, s_end, s_start_chord, c1, c2, c3;
     int origin_x, origin_y;
 };
@@ -527,9 +545,9 @@ __device__ __forceinline__ RaySegment interpolate_segment(
         const float lower = __fmaf_rn(__fsub_rn(v11, v01), tx, v01);
         seg[k] = __fmaf_rn(__fsub_rn(lower, upper), ty, upper);
     }
-    return RaySegment{seg[0],  seg[1],  seg[2],  seg[3],  seg[4],    seg[5],   seg[6],
-                      seg[7],  seg[8],  seg[9],  seg[10], seg[11],   seg[12],  seg[13],
-                      seg[14], seg[15], origin[0], origin[1]};
+    return RaySegment{pair(seg[0], seg[1]), pair(seg[2], seg[6]), pair(seg[3], seg[7]),
+                      pair(seg[4], seg[8]), pair(seg[5], seg[9]), seg[10], seg[11],
+                      seg[12], seg[13], seg[14], seg[15], origin[0], origin[1]};
 }
 
 // The state of one ray within one DEM pass of hierarchy_maximum.
@@ -604,23 +622,24 @@ __device__ __forceinline__ bool march_step_tracked(const Table &table, const Dem
     {
         if (kCount) ++steps;
         const float delta = __fsub_rn(s, g.s_start);
+        const float2 d1 = pair(delta, delta);
+        const float2 d2 = __fmul2_rn(d1, d1);
+        const float2 d3 = __fmul2_rn(d2, d1);
+        const float2 d4 = __fmul2_rn(d2, d2);
         // Relative arithmetic: offsets along the ray without the start, added
         // to the start relative to the origin; the absolute position (origin
         // + offset, rounded) only takes the bounds decisions.
-        float rx, ry, ux, uy, px, py;
+        float2 r, u, p;
         if (relative) {
-            rx = quartic(0.0f, g.a1, g.a2, g.a3, g.a4, delta);
-            ry = quartic(0.0f, g.b1, g.b2, g.b3, g.b4, delta);
-            ux = __fadd_rn(g.start_x, rx);
-            uy = __fadd_rn(g.start_y, ry);
-            px = __fadd_rn(static_cast<float>(g.origin_x), ux);
-            py = __fadd_rn(static_cast<float>(g.origin_y), uy);
+            r = quartic2(pair(0.0f, 0.0f), g.k1, g.k2, g.k3, g.k4, d1, d2, d3, d4);
+            u = __fadd2_rn(g.start, r);
+            p = __fadd2_rn(pair(static_cast<float>(g.origin_x), static_cast<float>(g.origin_y)),
+                           u);
         } else {
-            px = quartic(g.start_x, g.a1, g.a2, g.a3, g.a4, delta);
-            py = quartic(g.start_y, g.b1, g.b2, g.b3, g.b4, delta);
-            ux = px;
-            uy = py;
+            p = quartic2(g.start, g.k1, g.k2, g.k3, g.k4, d1, d2, d3, d4);
+            u = p;
         }
+        const float ux = u.x, uy = u.y, px = p.x, py = p.y;
         // NaN fails every comparison, as the reference's isnan tests do.
         if (!(px >= 0.0f && py >= 0.0f && px < last_x && py < last_y)) return false;
         const bool near = s < 0.5f;
@@ -629,17 +648,14 @@ __device__ __forceinline__ bool march_step_tracked(const Table &table, const Dem
             true_m = __fmul_rn(s, 1000.0f);
         } else {
             // The planar distance only feeds the far-field chord.
-            if (!relative) {
-                rx = __fsub_rn(px, g.start_x);
-                ry = __fsub_rn(py, g.start_y);
-            }
-            const float planar_x = __fmul_rn(rx, resolution);
-            const float planar_y = __fmul_rn(ry, resolution);
-            const float planar_m = hypot_fused(planar_x, planar_y);
+            if (!relative) r = sub2(p, g.start);
+            const float2 planar = __fmul2_rn(r, pair(resolution, resolution));
+            const float planar_m = hypot_fused(planar.x, planar.y);
             const float pm2 = __fmul_rn(planar_m, planar_m);
-            const float pm3 = __fmul_rn(pm2, planar_m);
-            float chord = __fmaf_rn(g.c1, planar_m, __fmul_rn(g.c2, pm2));
-            chord = __fmaf_rn(g.c3, pm3, chord);
+            // (c2 * pm2, pm2 * planar_m) in one instruction.
+            const float2 terms = __fmul2_rn(pair(g.c2, pm2), pair(pm2, planar_m));
+            float chord = __fmaf_rn(g.c1, planar_m, terms.x);
+            chord = __fmaf_rn(g.c3, terms.y, chord);
             true_m = __fmaf_rn(g.s_start_chord, 1000.0f, chord);
         }
         const float footprint = __fmul_rn(true_m, 0.004363323129985824f);
@@ -658,8 +674,8 @@ __device__ __forceinline__ bool march_step_tracked(const Table &table, const Dem
             side_here = level > 0 ? table.side(level) : -INFINITY;
         }
         // The tangent and its reciprocals depend only on delta.
-        const float dx = quartic_tangent(g.a1, g.a2, g.a3, g.a4, delta);
-        const float dy = quartic_tangent(g.b1, g.b2, g.b3, g.b4, delta);
+        const float2 tangent = quartic_tangent2(g.k1, g.k2, g.k3, g.k4, d1, d2, d3);
+        const float dx = tangent.x, dy = tangent.y;
         const float inv_x = fabsf(dx) > 1e-8f ? __frcp_rn(dx) : 1e30f;
         const float inv_y = fabsf(dy) > 1e-8f ? __frcp_rn(dy) : 1e30f;
         const int origin_x = relative ? g.origin_x : 0;

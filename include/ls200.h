@@ -394,6 +394,13 @@ ls200_status ls200_sun_loss_checkpoints(ls200_context *ctx, float *points, uint8
  * counterpart. */
 ls200_status ls200_fp32_probe(ls200_context *ctx, int iterations, double *tflops);
 
+/* Exhaustive check of the march's correctly rounded reciprocal (a hardware
+ * approximation plus one Newton-Raphson correction) against the IEEE
+ * round-to-nearest reciprocal on this device, over every 32-bit pattern with
+ * |x| >= 2^-64, both signs: `mismatches` = results that differ in any bit
+ * (must be 0), `checked` = results compared.  No reference counterpart. */
+ls200_status ls200_check_arithmetic(ls200_context *ctx, int64_t *mismatches, int64_t *checked);
+
 /* Device memory held by this library's own allocations on `device` (DEMs,
  * vector tables, context buffers; not the caller's buffers): bytes in use now
  * and the high-water mark since load or the last reset; reset_peak != 0 sets

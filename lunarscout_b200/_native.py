@@ -122,6 +122,7 @@ SIGNATURES: dict[str, list] = {
     "ls200_host_alloc": [_i64, _vp],
     "ls200_host_free": [_vp],
     "ls200_fp32_probe": [_vp, _i, _vp],
+    "ls200_check_arithmetic": [_vp, _vp, _vp],
 }
 _RESTYPES = {"ls200_last_error": ctypes.c_char_p, "ls200_abi_version": ctypes.c_int}
 

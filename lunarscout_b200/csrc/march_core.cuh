@@ -89,6 +89,19 @@ __device__ __forceinline__ void add_counters(unsigned long long *counters, unsig
     }
 }
 
+// Correctly rounded reciprocal: the hardware approximation plus one
+// Newton-Raphson correction whose residual an FMA forms exactly,
+// y' = y + y (1 - x y) with y ~ 1/x (P. W. Markstein, "Computation of
+// elementary functions on the IBM RISC System/6000 processor", IBM J. Res.
+// Develop. 34(1), 1990).  For 2^-64 <= |x| < 2^64 it equals __frcp_rn bit for
+// bit; |x| >= 2^64, infinities and NaN take __frcp_rn itself.
+// ls200_check_arithmetic compares every pattern with |x| >= 2^-64.
+__device__ __forceinline__ float rcp_approx(float x) {
+    float y;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+
 __device__ __forceinline__ float hypot_fused(float a, float b) {
     return __fsqrt_rn(__fmaf_rn(a, a, __fmul_rn(b, b)));
 }
@@ -140,6 +153,17 @@ __device__ __forceinline__ float2 quartic2(float2 x0, float2 k1, float2 k2, floa
     r = __ffma2_rn(k2, d2, r);
     r = __ffma2_rn(k3, d3, r);
     return __ffma2_rn(k4, d4, r);
+}
+
+// The correctly rounded reciprocal of both lanes (see rcp_approx), the
+// Newton step issued as f32x2 pairs; each lane needs |x| >= 2^-64.
+__device__ __forceinline__ float2 reciprocal_pair(float2 x) {
+    float2 y = pair(rcp_approx(x.x), rcp_approx(x.y));
+    const float2 e = __ffma2_rn(__fmul2_rn(x, pair(-1.0f, -1.0f)), y, pair(1.0f, 1.0f));
+    y = __ffma2_rn(y, e, y);
+    if (!(fabsf(x.x) < 0x1p64f)) y.x = __frcp_rn(x.x);
+    if (!(fabsf(x.y) < 0x1p64f)) y.y = __frcp_rn(x.y);
+    return y;
 }
 
 // Its derivative: a1 + 2 a2 d + 3 a3 d^2 + 4 a4 d^3 per lane
@@ -676,8 +700,10 @@ __device__ __forceinline__ bool march_step_tracked(const Table &table, const Dem
         // The tangent and its reciprocals depend only on delta.
         const float2 tangent = quartic_tangent2(g.k1, g.k2, g.k3, g.k4, d1, d2, d3);
         const float dx = tangent.x, dy = tangent.y;
-        const float inv_x = fabsf(dx) > 1e-8f ? __frcp_rn(dx) : 1e30f;
-        const float inv_y = fabsf(dy) > 1e-8f ? __frcp_rn(dy) : 1e30f;
+        // |d| > 1e-8 > 2^-64 wherever the Newton reciprocal is used.
+        const float2 reciprocal = reciprocal_pair(tangent);
+        const float inv_x = fabsf(dx) > 1e-8f ? reciprocal.x : 1e30f;
+        const float inv_y = fabsf(dy) > 1e-8f ? reciprocal.y : 1e30f;
         const int origin_x = relative ? g.origin_x : 0;
         const int origin_y = relative ? g.origin_y : 0;
         const int ipx = relative ? origin_x + static_cast<int>(floorf(ux)) : static_cast<int>(px);

@@ -411,6 +411,15 @@ class CudaSession:
         call("ls200_get_batch_config", self._ctx, *[ctypes.byref(v) for v in values])
         return BatchConfig(*(v.value for v in values))
 
+    def check_arithmetic(self) -> tuple[int, int]:
+        """(mismatches, checked): results of the march's Newton reciprocal
+        that differ in any bit from the IEEE reciprocal, over every pattern
+        with |x| >= 2^-64 and both signs; mismatches must be 0."""
+        mismatches, checked = ctypes.c_int64(), ctypes.c_int64()
+        call("ls200_check_arithmetic", self._ctx, ctypes.byref(mismatches),
+             ctypes.byref(checked))
+        return int(mismatches.value), int(checked.value)
+
     def fp32_probe(self, iterations: int = 4096) -> float:
         """Measured FP32 FMA throughput of this device in TFLOP/s."""
         value = ctypes.c_double()

@@ -41,11 +41,12 @@ struct SharedLevels {
     __device__ __forceinline__ int4 cells(int l) const { return t.cells[l]; }
 };
 
-// Resident 128-thread blocks per SM the register budget is sized for: 10
-// (51 registers, a few bytes of spills) marched 1-2 % faster than 8 (64
-// registers, none) with the 4-pixel lane layout; 12 was slower.
+// Resident 128-thread blocks per SM the register budget is sized for.  With
+// the f32x2 pairs and the Newton reciprocal, 9 (56 registers) marched 3.9 %
+// faster than 10 (48 registers, whose spills had grown) and 3.6 % faster than
+// 8 (64 registers) on site-scale tiles; 12 was slower.
 #ifndef LS_MARCH_MIN_BLOCKS
-#define LS_MARCH_MIN_BLOCKS 10
+#define LS_MARCH_MIN_BLOCKS 9
 #endif
 // Adjacent pixels of one azimuth in a warp (a power of two up to 32); the
 // warp's other lanes take the next azimuths of the same pixels.  4 pixels x

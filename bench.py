@@ -61,16 +61,22 @@ def log(*args):
     print(*args, file=sys.stderr, flush=True)
 
 
-def profiled_traffic(name: str):
-    """DRAM bytes per launch recorded by the committed ncu summary, if any."""
+def profiled_value(name: str, key: str):
+    """A `key: value` figure recorded by a committed ncu summary, if any."""
     path = ROOT / "profiles" / name
     try:
         for line in path.read_text().splitlines():
-            if line.startswith("dram_bytes_per_launch:"):
-                return int(line.split(":", 1)[1])
-    except OSError:
+            if line.startswith(key + ":"):
+                return float(line.split(":", 1)[1])
+    except (OSError, ValueError):
         return None
     return None
+
+
+def profiled_traffic(name: str):
+    """DRAM bytes per launch recorded by the committed ncu summary, if any."""
+    value = profiled_value(name, "dram_bytes_per_launch")
+    return None if value is None else int(value)
 
 
 def max_over_ranks(value: float, world: int, device: str = "cuda") -> float:
@@ -1409,6 +1415,12 @@ def run_ours(args):
                 "node_visits_per_ray": visits / (args.steps * RAYS_PER_TILE),
                 "ray_steps_per_ray": ray_steps / (args.steps * RAYS_PER_TILE),
                 "level0_samples_per_ray": samples / (args.steps * RAYS_PER_TILE),
+                # The march is bound by instruction issue, not by FP32 FMA
+                # throughput: the share of issue slots its launch keeps busy.
+                "issue_slots_busy": profiled_value("march_pass_kernel_site_tile.md",
+                                                   "issue_slots_busy"),
+                "issue_source": "ncu smsp__issue_active.avg.pct_of_peak_sustained_active of "
+                                "one pass-0 launch (profiles/march_pass_kernel_site_tile.md)",
             },
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": "rays/s", "h2d_bytes_per_step": h2d,

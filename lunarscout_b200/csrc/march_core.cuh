@@ -155,12 +155,19 @@ __device__ __forceinline__ float2 quartic2(float2 x0, float2 k1, float2 k2, floa
     return __ffma2_rn(k4, d4, r);
 }
 
-// The correctly rounded reciprocal of both lanes (see rcp_approx), the
-// Newton step issued as f32x2 pairs; each lane needs |x| >= 2^-64.
-__device__ __forceinline__ float2 reciprocal_pair(float2 x) {
-    float2 y = pair(rcp_approx(x.x), rcp_approx(x.y));
+// The Newton reciprocal of both lanes without the range fallback (the
+// caller handles |x| >= 2^64).
+__device__ __forceinline__ float2 newton_reciprocal_pair(float2 x) {
+    const float2 y = pair(rcp_approx(x.x), rcp_approx(x.y));
     const float2 e = __ffma2_rn(__fmul2_rn(x, pair(-1.0f, -1.0f)), y, pair(1.0f, 1.0f));
-    y = __ffma2_rn(y, e, y);
+    return __ffma2_rn(y, e, y);
+}
+
+// The correctly rounded reciprocal of both lanes (see rcp_approx), the
+// Newton step issued as f32x2 pairs; each lane needs |x| >= 2^-64.  The
+// march inlines the same choice with one branch for both lanes.
+__device__ __forceinline__ float2 reciprocal_pair(float2 x) {
+    float2 y = newton_reciprocal_pair(x);
     if (!(fabsf(x.x) < 0x1p64f)) y.x = __frcp_rn(x.x);
     if (!(fabsf(x.y) < 0x1p64f)) y.y = __frcp_rn(x.y);
     return y;
@@ -700,10 +707,17 @@ __device__ __forceinline__ bool march_step_tracked(const Table &table, const Dem
         // The tangent and its reciprocals depend only on delta.
         const float2 tangent = quartic_tangent2(g.k1, g.k2, g.k3, g.k4, d1, d2, d3);
         const float dx = tangent.x, dy = tangent.y;
-        // |d| > 1e-8 > 2^-64 wherever the Newton reciprocal is used.
-        const float2 reciprocal = reciprocal_pair(tangent);
-        const float inv_x = fabsf(dx) > 1e-8f ? reciprocal.x : 1e30f;
-        const float inv_y = fabsf(dy) > 1e-8f ? reciprocal.y : 1e30f;
+        // The Newton reciprocal is exact for 2^-64 <= |d| < 2^64 and used only
+        // for |d| > 1e-8; a tangent of 2^64 or more (or not finite) takes the
+        // IEEE reciprocal on a branch of its own.
+        const float2 newton = newton_reciprocal_pair(tangent);
+        const float ax = fabsf(dx), ay = fabsf(dy);
+        float inv_x = ax > 1e-8f ? newton.x : 1e30f;
+        float inv_y = ay > 1e-8f ? newton.y : 1e30f;
+        if (!(ax < 0x1p64f && ay < 0x1p64f)) {
+            inv_x = ax > 1e-8f ? __frcp_rn(dx) : 1e30f;
+            inv_y = ay > 1e-8f ? __frcp_rn(dy) : 1e30f;
+        }
         const int origin_x = relative ? g.origin_x : 0;
         const int origin_y = relative ? g.origin_y : 0;
         const int ipx = relative ? origin_x + static_cast<int>(floorf(ux)) : static_cast<int>(px);

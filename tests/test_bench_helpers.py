@@ -55,3 +55,16 @@ def test_reference_arm_steps_are_measured(monkeypatch, capsys):
     assert line["ms_per_step"] == 500.0
     assert line["value"] == bench.REFERENCE_STEP_RAYS / 0.5
     assert line["cpu_baseline"]["cores"] == 4
+
+
+def test_roofline_reads_the_committed_ncu_summary():
+    """The bench's roofline takes the DRAM traffic and the issue-slot share of
+    the march from the committed ncu summary of the same workload."""
+    import bench
+
+    traffic = bench.profiled_traffic("march_pass_kernel_site_tile.md")
+    busy = bench.profiled_value("march_pass_kernel_site_tile.md", "issue_slots_busy")
+    assert traffic is not None and 1e8 < traffic < 1e9
+    assert busy is not None and 0.5 < busy <= 1.0
+    assert bench.profiled_value("march_pass_kernel_site_tile.md", "no_such_key") is None
+    assert bench.profiled_traffic("no_such_summary.md") is None

@@ -106,15 +106,20 @@ constexpr float kTwoPi = 6.283185307179586f;      // float32(2 pi)
 
 // Azimuth (deg, [0, 360)) and elevation (deg) of a float32 Moon-ME vector in
 // a pixel's frame (lightmap_cpu.py:105-120).
+// The east and north components are computed as one f32x2 pair (sm_100),
+// each lane rounding as the scalar __fmul_rn / __fadd_rn does.
 __device__ __forceinline__ void body_direction(const Frame32 &f, float vx, float vy, float vz,
                                                float &azimuth_deg, float &elevation) {
-    const float ex = __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(vx, f.v[0]), __fmul_rn(vy, f.v[3])),
-                                         __fmul_rn(vz, f.v[6])), f.v[9]);
-    const float ey = __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(vx, f.v[1]), __fmul_rn(vy, f.v[4])),
-                                         __fmul_rn(vz, f.v[7])), f.v[10]);
+    const float2 xy = __fadd2_rn(
+        __fadd2_rn(__fadd2_rn(__fmul2_rn(make_float2(vx, vx), make_float2(f.v[0], f.v[1])),
+                              __fmul2_rn(make_float2(vy, vy), make_float2(f.v[3], f.v[4]))),
+                   __fmul2_rn(make_float2(vz, vz), make_float2(f.v[6], f.v[7]))),
+        make_float2(f.v[9], f.v[10]));
+    const float ex = xy.x, ey = xy.y;
     const float ez = __fadd_rn(__fadd_rn(__fadd_rn(__fmul_rn(vx, f.v[2]), __fmul_rn(vy, f.v[5])),
                                          __fmul_rn(vz, f.v[8])), f.v[11]);
-    const float horizontal = __fsqrt_rn(__fadd_rn(__fmul_rn(ex, ex), __fmul_rn(ey, ey)));
+    const float2 squares = __fmul2_rn(xy, xy);
+    const float horizontal = __fsqrt_rn(__fadd_rn(squares.x, squares.y));
     elevation = __fmul_rn(atan2f(ez, horizontal), kRadToDeg);
     float azimuth = atan2f(ex, ey);
     if (azimuth < 0.0f) azimuth = __fadd_rn(azimuth, kTwoPi);

@@ -115,7 +115,13 @@ ls200_status ls200_march_all_passes(ls200_context *ctx, const float *segments,
                                     double *pass_seconds);
 /* Device-resident variant: device_segments in, device_slopes out
  * ([P, A] pixel-major slopes, or degrees when `degrees` is non-zero);
- * pass_seconds as above (NULL skips the per-pass events and the wait). */
+ * pass_seconds as above (NULL skips the per-pass events and the wait).
+ * The host-segment entry points refuse segments on which the FP32 path
+ * position would stop moving (s_end of 2048 km or more, or a pixel too small
+ * for the ray length: the reference's kernel would never end there either);
+ * ls200_segments_device refuses the same through its distance limit.  Device
+ * segments given here are not read back: they must come from
+ * ls200_segments_device or satisfy the same limits. */
 ls200_status ls200_march_all_passes_device(ls200_context *ctx, const float *device_segments,
                                            int azimuth_count, int center_count,
                                            int dem_count, ls200_dem *const *dems,

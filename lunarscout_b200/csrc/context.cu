@@ -1,6 +1,7 @@
 // Context lifecycle, error plumbing and device-resident DEMs of the ls200 C ABI.
 #include "internal.cuh"
 
+#include <cmath>
 #include <vector>
 
 namespace ls200 {
@@ -32,6 +33,25 @@ int pyramid_layout(int width, int height, PyramidLevel *levels, int capacity,
     }
     if (mip_count) *mip_count = offset;
     return count;
+}
+
+double dem_resolution_m(const ls200_dem *dem) {
+    const float *m = dem->map_parameters;
+    return 0.5 * (std::hypot(double(m[6]), double(m[9])) + std::hypot(double(m[7]), double(m[10])));
+}
+
+void require_march_progress(double s_end_km, const ls200_dem *active) {
+    if (!(s_end_km > 0.0)) return;  // no segment reaches past its start
+    LS_REQUIRE(s_end_km < 2048.0,
+               "rays longer than 2048 km cannot be marched in FP32 (the position would stop "
+               "moving)");
+    int exponent = 0;
+    std::frexp(s_end_km, &exponent);  // s_end_km = f * 2^exponent, f in [0.5, 1)
+    const double ulp_km = std::ldexp(1.0, exponent - 24);
+    const double resolution = dem_resolution_m(active);
+    LS_REQUIRE(std::isfinite(resolution) && resolution * 0.5e-3 > 2.0 * ulp_km,
+               "the DEM's pixel size is too small for rays of this length (the FP32 position "
+               "would stop moving)");
 }
 
 }  // namespace ls200

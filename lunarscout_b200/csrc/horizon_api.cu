@@ -73,6 +73,19 @@ void slopes_to_degrees_device(ls200_context *ctx, const float *slopes, int64_t c
     LS_CUDA(cudaGetLastError());
 }
 
+// The largest finite s_end (km, field 13) of pass `pass` in host segments
+// [A, C, D, 18].
+static double host_segment_end_km(const float *segments, int azimuth_count, int center_count,
+                                  int dem_count, int pass) {
+    double end = 0.0;
+    const size_t rays = static_cast<size_t>(azimuth_count) * center_count;
+    for (size_t r = 0; r < rays; ++r) {
+        const float value = segments[(r * dem_count + pass) * kSegmentFields + 13];
+        if (value > end) end = value;  // NaN never compares greater
+    }
+    return end;
+}
+
 static void check_tile(int azimuth_count, int center_count, int dem_count, int tile_width,
                        int tile_height, int subpatch) {
     LS_REQUIRE(azimuth_count > 0 && dem_count > 0, "segment dimensions must be positive");
@@ -150,6 +163,9 @@ ls200_status ls200_march_pass(ls200_context *ctx, const float *segments, int azi
         LS_REQUIRE(pass_index >= 0 && pass_index < dem_count,
                    "pass_index is outside the segment DEM axis");
         LS_REQUIRE(active->level_count <= kMaxLevels, "active pyramid is too deep");
+        require_march_progress(host_segment_end_km(segments, azimuth_count, center_count,
+                                                   dem_count, pass_index),
+                               active);
         std::lock_guard<std::mutex> hold(ctx->lock);
         activate(ctx);
         const int pixel_count = tile_width * tile_height;
@@ -192,7 +208,11 @@ ls200_status ls200_march_all_passes(ls200_context *ctx, const float *segments,
         LS_REQUIRE(ctx && segments && dems && slopes, "NULL argument");
         check_tile(azimuth_count, center_count, dem_count, tile_width, tile_height,
                    subpatch_size);
-        for (int d = 0; d < dem_count; ++d) LS_REQUIRE(dems[d] != nullptr, "NULL DEM");
+        for (int d = 0; d < dem_count; ++d) {
+            LS_REQUIRE(dems[d] != nullptr, "NULL DEM");
+            require_march_progress(
+                host_segment_end_km(segments, azimuth_count, center_count, dem_count, d), dems[d]);
+        }
         std::lock_guard<std::mutex> hold(ctx->lock);
         activate(ctx);
         const size_t n = static_cast<size_t>(tile_width) * tile_height * azimuth_count;

@@ -174,6 +174,17 @@ void sanitize_level0(ls200_context *ctx, ls200_dem *dem);
 // Write dem->bounds from dem->cells (after both parts of cells are final).
 void build_cell_bounds(ls200_context *ctx, ls200_dem *dem);
 
+// Mean pixel size (m) of a DEM from its map parameters, in FP64.
+double dem_resolution_m(const ls200_dem *dem);
+// Refuses a march whose rays would step in place.  The march (like the
+// reference's kernel) advances its FP32 path position s (km) by at least
+// 1e-4 km per cull and at least half a pixel per level-0 sample; each must
+// exceed half an ulp of s, or s stops moving and the ray never ends.  Below
+// 2048 km the cull advance always does; the sample advance, half a pixel of
+// the active DEM, is required to exceed 2 ulp(s_end_km) (a factor four of
+// margin).
+void require_march_progress(double s_end_km, const ls200_dem *active);
+
 // Segment generation into device memory.
 void segments_device(ls200_context *ctx, ls200_dem *const *dems, int dem_count,
                      int tile_column, int tile_row, int tile_width, int azimuth_count,

@@ -390,6 +390,9 @@ void segments_device(ls200_context *ctx, ls200_dem *const *dems, int dem_count,
     P.segments = device_segments;
     for (int d = 0; d < dem_count; ++d) {
         P.dem = make_dem(dems[d], maximum_distance_m);
+        // A segment ends within the DEM's ray limit (the path is at most a
+        // few percent longer than the chord).
+        require_march_progress(P.dem.ray_limit * 1.05e-3 + 1.0, dems[d]);
         P.dem_index = d;
         segments_kernel<<<(jobs + 127) / 128, 128, 0, ctx->stream>>>(P);
         LS_CUDA(cudaGetLastError());

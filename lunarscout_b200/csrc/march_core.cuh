@@ -14,10 +14,13 @@
 //     dist*dist - local_z^2, which fuses local_z^2.
 // That is the reference's Numba-CUDA kernel as NVVM compiles it on the B200
 // (its slopes on the same GPU are the golden file numba_cuda_b200.npz of the
-// tests).  Division, reciprocal and square root are IEEE round-to-nearest.
+// tests).  Division, reciprocal and square root are IEEE round-to-nearest;
+// the tangent's reciprocals come from rcp.approx plus one Newton step, which
+// equals the IEEE reciprocal on every input it receives (see rcp_approx).
 // The x and y arithmetic of a step (path position and tangent, planar
 // offset, cell-exit slab) is issued as f32x2 pairs, whose lanes round as the
-// scalar intrinsics do.
+// scalar intrinsics do.  No shift amount is ever taken from stored state:
+// an amount out of range is undefined even on a path that is never taken.
 // With the same segment inputs the results are bit-identical to the CPU
 // oracle's FP32 restatement under its production mask.
 //

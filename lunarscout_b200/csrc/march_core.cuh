@@ -378,7 +378,7 @@ __device__ __forceinline__ float cell_bound(const float *__restrict__ bounds, in
 }
 
 // Advance (km) to the exit of the cell (cx, cy) of side 4^level pixels along
-// the tangent, + 1e-4 km, or `fallback` when the exit is not ahead
+// the tangent, or `fallback` when the exit is not ahead, + 1e-4 km
 // (cuda_backend.py:733-762).  Of max(t1, t2) only the far edge can win:
 // (min_x - px) <= 0 < (max_x - px), so the product with inv_x keeps that
 // order's sign pattern and the larger t is the edge ahead of the ray
@@ -396,8 +396,12 @@ __device__ __forceinline__ float cell_exit_advance(int shift, int cx, int cy, fl
     const float2 tm = __fmul2_rn(sub2(edge, pair(ux, uy)), pair(inv_x, inv_y));
     const float tmx = tm.x, tmy = tm.y;
     const float exit_distance = tmx < tmy ? tmx : tmy;
-    const float to_exit = exit_distance > 0.0f ? exit_distance : fallback;
-    return to_exit > 0.0f ? __fadd_rn(to_exit, 0.0001f) : fallback;
+    // The reference returns `fallback` when the distance it adds 1e-4 km to
+    // is not positive; that distance is the exit or, behind the ray, the
+    // fallback, which is positive on every DEM that marches (the host
+    // refuses pixel sizes too small for the ray length).  With a fallback of
+    // zero the reference would not advance and its ray would never end.
+    return __fadd_rn(exit_distance > 0.0f ? exit_distance : fallback, 0.0001f);
 }
 
 // The skip ladder.  After a cull at `level`, climb to the ancestors of the
